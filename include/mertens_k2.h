@@ -1,0 +1,87 @@
+/*
+ * mertens_k2.h -- C-ABI of libmertens_k2.so, the B200 (sm_100a) evaluator of
+ *
+ *   K2(v, T, k) = 2 sum_{0<gamma<T} exp(-k gamma^2) Re( e^{i gamma v} / (rho zeta'(rho)) ),
+ *   rho = 1/2 + i gamma,
+ *
+ * the zero sum of bzyzz/mertens_bound (README.md:28, THEOREM.md:7).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Host-pointer entry points copy in and out on the
+ *     table's own CUDA stream and return after the results are on the host.  *_dev entry
+ *     points take device pointers and a cudaStream_t passed as void* and return without
+ *     synchronising.
+ *   - Every entry point returns an int status: MB_OK (0) or a negative MB_ERR_* code;
+ *     mb_last_error() gives a message for the calling thread.  No entry point exits the
+ *     process.  (The reference's evaluator has no error channel at all:
+ *     search/path1_eval_fast.cpp:15,58 return void and check nothing.)
+ *   - G_j = gamma_j / 2pi is unsigned 64.128 fixed point, passed as three u64 limbs per zero
+ *     in the order [integer, fraction hi, fraction lo] (row-major n x 3).  The integer part
+ *     must be < 2^32.
+ *   - A candidate point is v = v_int + v_frac 2^-64 (+ an optional FP64 offset delta).
+ *   - The cutoff T keeps the zeros with gamma_j < T (the table is sorted, so these are the
+ *     first count_below(T) zeros); T = +inf keeps them all.
+ *   - Outputs: val = K2, dd = dK2/ddelta (= dK2/dv), dk = dK2/dk.
+ *   - A table handle must not be used by two host threads at the same time.
+ */
+#ifndef MERTENS_K2_H
+#define MERTENS_K2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MB_OK 0
+#define MB_ERR_ARG (-1)      /* bad argument: null pointer, size or value out of range      */
+#define MB_ERR_TABLE (-2)    /* table data rejected: unsorted gamma, non-finite c, G/gamma   */
+#define MB_ERR_CUDA (-3)     /* CUDA runtime error                                          */
+#define MB_ERR_TIMEOUT (-4)  /* a bounded device-side wait gave up                          */
+#define MB_ERR_STATE (-5)    /* call made in the wrong state (e.g. plan for another table)  */
+#define MB_ERR_CAPACITY (-6) /* request larger than a fixed capacity                        */
+
+typedef struct mb_table mb_table;
+
+/* Message for the last failed call on this thread ("" if none). */
+const char *mb_last_error(void);
+
+/* ABI version of this library (bumped on any signature change). */
+int mb_abi_version(void);
+
+/* Upload a zero table to device `device` and validate it.
+ * Replaces the table loading of search/eval_tech1_600k.py:38-50 (load_zeros_bin) and
+ * search/gpu_mertens_stream.cu:298-379 (ZeroData::load) -- those read a file; this takes the
+ * arrays (the file formats are read by the Python host layer).
+ * Rejected with MB_ERR_TABLE: gamma not strictly increasing or not finite/positive,
+ * non-finite c, G integer part >= 2^32, or |gamma - 2pi G| > 4 ulp(gamma). */
+int mb_table_create(const uint64_t *G3, const double *c_re, const double *c_im, const double *gamma,
+                    int64_t n, int device, mb_table **out);
+int mb_table_destroy(mb_table *t);
+int mb_table_size(const mb_table *t, int64_t *n_out);
+/* Number of zeros with gamma < T. */
+int mb_table_count_below(const mb_table *t, double T, int64_t *n_out);
+
+/* Exact phase floor(frac(v G_j) 2^128) for every candidate and the first n_zeros zeros,
+ * written row-major (P x n_zeros) as (hi, lo) words.  The hi word is floor(frac(v G) 2^64).
+ * The reduction restated: search/path1_eval_fast.cpp:41-46 (128-bit fixed-point product,
+ * top word kept) and legacy/superseded/certify_peak2_600k.py:183-187. */
+int mb_phase128(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                int64_t n_zeros, uint64_t *out_hi, uint64_t *out_lo);
+
+/* Plain FP64 evaluation of K2 and its gradient: exact integer phase reduction, FP64
+ * sine/cosine, FP64 accumulation.
+ * Replaces search/path1_eval_fast.cpp:15-53 followed by the h0 sum at :76-81 (compute_peak_AB
+ * then sum w A), and the term loop of certification/certify_K2.py:116-121 (point value). */
+int mb_k2_plain(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                const double *delta, double k, double T, double *out_val, double *out_dd,
+                double *out_dk);
+int mb_k2_plain_dev(mb_table *t, int64_t P, const uint64_t *d_v_int, const uint64_t *d_v_frac,
+                    const double *d_delta, double k, double T, double *d_val, double *d_dd,
+                    double *d_dk, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MERTENS_K2_H */

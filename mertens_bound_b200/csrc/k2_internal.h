@@ -1,0 +1,100 @@
+// Host-side internals of libmertens_k2.so (not part of the public C-ABI).
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "../../include/mertens_k2.h"
+
+namespace mb {
+
+// Thread-local last-error message (mb_last_error()).
+void set_error(const char *fmt, ...);
+const char *last_error();
+
+// Return-on-error helpers used by every entry point.
+#define MB_CHECK_ARG(cond, ...)                          \
+    do {                                                 \
+        if (!(cond)) {                                   \
+            ::mb::set_error(__VA_ARGS__);                \
+            return MB_ERR_ARG;                           \
+        }                                                \
+    } while (0)
+
+#define MB_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            ::mb::set_error("CUDA error %s (%s) at %s:%d", cudaGetErrorName(e_),            \
+                            cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+            return MB_ERR_CUDA;                                                             \
+        }                                                                                   \
+    } while (0)
+
+#define MB_TRY(call)              \
+    do {                          \
+        int s_ = (call);          \
+        if (s_ != MB_OK) return s_; \
+    } while (0)
+
+// Grow-only device buffer.  ensure() synchronises the device before it frees a smaller
+// buffer, so work still in flight on any stream never sees its memory released.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t need);
+    void release();
+};
+
+// Device-resident zero table.  Planar (structure of arrays), every array 256-byte aligned:
+//   g[0..4][n]  u32 limbs of G 2^128 (g0 least significant .. g4 = integer part)
+//   gamma[n], c_re[n], c_im[n]    FP64 as given
+//   alpha[n] = |c|, psi[n] = round(frac(arg(c)/2pi) 2^64)   (derived at creation)
+struct Table {
+    int device = 0;
+    int64_t n = 0;
+    uint32_t *d_g = nullptr;          // 5*n words, limb-major
+    double *d_gamma = nullptr, *d_cre = nullptr, *d_cim = nullptr;
+    double *d_alpha = nullptr;
+    uint64_t *d_psi = nullptr;
+    std::vector<double> h_gamma;      // host copies for cutoffs and error planning
+    std::vector<double> h_alpha;
+    cudaStream_t stream = nullptr;    // the library's own stream for host-pointer calls
+    // grow-only scratch owned by the table: `io` stages candidates and results of host-pointer
+    // calls, `work` holds per-chunk partial sums.  Calls on one table must not overlap on the GPU.
+    DevBuf io, work;
+
+    int64_t count_below(double T) const;
+};
+
+// Device view of the table passed to kernels by value.
+struct TabView {
+    const uint32_t *g0, *g1, *g2, *g3, *g4;
+    const double *gamma, *cre, *cim, *alpha;
+    const uint64_t *psi;
+    int64_t n;
+};
+
+TabView view(const Table &t);
+
+// Candidate arrays on the device.
+struct CandView {
+    const uint64_t *vi, *vf;
+    const double *delta;   // may be null (all zero)
+    int64_t P;
+};
+
+int device_guard(int device);
+
+// Kernel launchers (return MB_OK or an MB_ERR_* code).
+Table &table_of(struct ::mb_table *h);
+
+int launch_phase128(const Table &t, CandView c, int64_t n_zeros, uint64_t *d_hi, uint64_t *d_lo,
+                    cudaStream_t s);
+int launch_plain(Table &t, CandView c, int64_t n_use, double k, double *d_val, double *d_dd,
+                 double *d_dk, cudaStream_t s, double *d_partial_override = nullptr,
+                 size_t partial_cap = 0);
+
+}  // namespace mb

@@ -1,0 +1,208 @@
+"""CPU oracle for the K2 evaluator -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference leg may
+import this module.  It is the checker, never the thing measured or shipped.
+
+Contents
+  * phase128_bigint     -- exact floor(frac(v G) 2^128) with Python integers (the definition).
+  * Oracle              -- binding of _build/liboracle.so (k2_oracle.c): exact phase and the
+                           K2 value/gradient sums in binary128.
+  * reference_format    -- the synthetic table and candidates in the reference's layout
+                           (search/path1_build_zeros_100k.py:102-104: ghi = rint(G 2^146) mod 2^128,
+                           glo = rint(G 2^98), psi = rint(((-arg c / 2pi) mod 1) 2^128), alpha = |c|;
+                           x = floor(v 2^30) as u128 with the remaining fraction in dy0,
+                           search/eval_tech1_600k.py:213-215).
+  * RefLib              -- binding of _ref/libpath1_eval.so, the reference's own evaluator
+                           compiled from search/path1_eval_fast.cpp (see Makefile).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libpath1_eval.so")
+MASK64 = (1 << 64) - 1
+MASK128 = (1 << 128) - 1
+
+
+def build() -> None:
+    """Compile the oracle (and the reference evaluator when its source is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True, capture_output=True)
+
+
+# ------------------------------------------------------------------ exact phase (definition)
+
+def phase128_bigint(vi: int, vf: int, g: tuple[int, int, int]) -> tuple[int, int]:
+    """floor(frac(v G) 2^128) for v = vi + vf 2^-64, G = g0 + g1 2^-64 + g2 2^-128."""
+    V = (int(vi) << 64) | int(vf)
+    Gf = (int(g[0]) << 128) | (int(g[1]) << 64) | int(g[2])
+    ph = ((V * Gf) >> 64) & MASK128
+    return ph >> 64, ph & MASK64
+
+
+# ------------------------------------------------------------------ C oracle
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Oracle:
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.orc_phase128.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_k2_quad.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+        L.orc_abs_sum.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
+        L.orc_abs_sum.restype = C.c_double
+        L.orc_gamma_from_G.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
+        L.orc_ref_peak_AB.argtypes = [C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 11
+        L.orc_ref_polish.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_double, C.c_int] + [C.c_void_p] * 3
+        self.L = L
+
+    def phase128(self, cands, G3, n=None):
+        vi = np.ascontiguousarray(cands.v_int, dtype=np.uint64)
+        vf = np.ascontiguousarray(cands.v_frac, dtype=np.uint64)
+        G3 = np.ascontiguousarray(G3 if n is None else G3[:n], dtype=np.uint64)
+        P, N = vi.shape[0], G3.shape[0]
+        hi = np.empty((P, N), dtype=np.uint64)
+        lo = np.empty((P, N), dtype=np.uint64)
+        self.L.orc_phase128(P, _p(vi), _p(vf), N, _p(G3), _p(hi), _p(lo))
+        return hi, lo
+
+    def k2(self, cands, table, k: float, n_use: int):
+        """(val, dd, dk) in binary128, returned as (P, 3) hi parts and (P, 3) lo parts."""
+        vi = np.ascontiguousarray(cands.v_int, dtype=np.uint64)
+        vf = np.ascontiguousarray(cands.v_frac, dtype=np.uint64)
+        d = np.ascontiguousarray(cands.delta, dtype=np.float64)
+        P = vi.shape[0]
+        out = np.empty((P, 6), dtype=np.float64)
+        G3 = np.ascontiguousarray(table.G3, dtype=np.uint64)
+        self.L.orc_k2_quad(P, _p(vi), _p(vf), _p(d), int(n_use), _p(G3), _p(np.ascontiguousarray(table.c_re)),
+                           _p(np.ascontiguousarray(table.c_im)), float(k), _p(out))
+        return out[:, 0::2].copy(), out[:, 1::2].copy()
+
+    def abs_sum(self, table, k: float, n_use: int) -> float:
+        return self.L.orc_abs_sum(int(n_use), _p(np.ascontiguousarray(table.G3)), _p(np.ascontiguousarray(table.c_re)),
+                                  _p(np.ascontiguousarray(table.c_im)), float(k))
+
+    def gamma_from_G(self, G3):
+        G3 = np.ascontiguousarray(G3, dtype=np.uint64)
+        g = np.empty(G3.shape[0])
+        self.L.orc_gamma_from_G(G3.shape[0], _p(G3), _p(g))
+        return g
+
+    def ref_peak_AB(self, refc, reft, n=None, want_top=False):
+        """Restated compute_peak_AB (single-threaded); refc/reft from reference_format()."""
+        x_lo, x_hi, dy0 = refc
+        n = reft["n"] if n is None else n
+        P = x_lo.shape[0]
+        A = np.empty((P, n)); B = np.empty((P, n))
+        top = np.empty((P, n), dtype=np.uint64) if want_top else None
+        self.L.orc_ref_peak_AB(P, _p(x_lo), _p(x_hi), _p(dy0), n, _p(reft["alpha"]), _p(reft["gamma"]),
+                               _p(reft["ghi_lo"]), _p(reft["ghi_hi"]), _p(reft["glo_lo"]), _p(reft["glo_hi"]),
+                               _p(reft["psi_lo"]), _p(reft["psi_hi"]), _p(A), _p(B),
+                               _p(top) if want_top else None)
+        return (A, B, top) if want_top else (A, B)
+
+    def ref_polish(self, A, B, gamma, w, half, steps):
+        P, n = A.shape
+        hu, hp, dp = np.empty(P), np.empty(P), np.empty(P)
+        self.L.orc_ref_polish(P, n, _p(np.ascontiguousarray(A)), _p(np.ascontiguousarray(B)),
+                              _p(np.ascontiguousarray(gamma[:n])), _p(np.ascontiguousarray(w[:n])),
+                              float(half), int(steps), _p(hu), _p(hp), _p(dp))
+        return hu, hp, dp
+
+
+# ------------------------------------------------------------------ reference layout adapter
+
+def _rint_shift(x: int, s: int) -> int:
+    """round-half-even(x / 2^s) for integers."""
+    q, r = x >> s, x & ((1 << s) - 1)
+    half = 1 << (s - 1)
+    if r > half or (r == half and (q & 1)):
+        q += 1
+    return q
+
+
+def reference_format(table, n=None):
+    """The table in the reference's zeros_600k.bin field set (planar arrays)."""
+    import mpmath as mp
+
+    n = table.G3.shape[0] if n is None else n
+    out = {k: np.empty(n, dtype=np.uint64) for k in ("ghi_lo", "ghi_hi", "glo_lo", "glo_hi", "psi_lo", "psi_hi")}
+    with mp.workprec(256):
+        two_pi = 2 * mp.pi
+        for j in range(n):
+            gi, g1, g2 = (int(x) for x in table.G3[j])
+            Gf = (gi << 128) | (g1 << 64) | g2
+            ghi = (Gf << 18) & MASK128                 # G 2^146 mod 2^128 (exact)
+            glo = _rint_shift(Gf, 30) & MASK128        # rint(G 2^98)
+            a = mp.atan2(mp.mpf(float(table.c_im[j])), mp.mpf(float(table.c_re[j])))
+            frac = (-a / two_pi) % 1
+            psi = int(mp.nint(frac * mp.mpf(2) ** 128)) & MASK128
+            out["ghi_lo"][j], out["ghi_hi"][j] = ghi & MASK64, ghi >> 64
+            out["glo_lo"][j], out["glo_hi"][j] = glo & MASK64, glo >> 64
+            out["psi_lo"][j], out["psi_hi"][j] = psi & MASK64, psi >> 64
+    out["alpha"] = np.ascontiguousarray(np.hypot(table.c_re[:n], table.c_im[:n]))
+    out["gamma"] = np.ascontiguousarray(table.gamma[:n])
+    out["n"] = n
+    return out
+
+
+def reference_candidates(cands):
+    """x = floor(v 2^30) (u128 as lo/hi words) and dy0 = v - x 2^-30 (+ delta), in FP64."""
+    P = cands.v_int.shape[0]
+    x_lo = np.empty(P, dtype=np.uint64); x_hi = np.empty(P, dtype=np.uint64); dy0 = np.empty(P)
+    for p in range(P):
+        vi, vf = int(cands.v_int[p]), int(cands.v_frac[p])
+        x = (vi << 30) | (vf >> 34)
+        x_lo[p], x_hi[p] = x & MASK64, x >> 64
+        dy0[p] = float(vf & ((1 << 34) - 1)) * 2.0**-64 + float(cands.delta[p])
+    return x_lo, x_hi, dy0
+
+
+# ------------------------------------------------------------------ reference evaluator
+
+class RefLib:
+    """The reference's compiled evaluator (compute_peak_AB, polish_peaks_with_weights)."""
+
+    def __init__(self):
+        if not os.path.exists(REF_SO):
+            build()
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(REF_SO)
+        L = C.CDLL(REF_SO)
+        L.compute_peak_AB.argtypes = [C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 10
+        L.compute_peak_AB.restype = None
+        L.polish_peaks_with_weights.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_double, C.c_int] + [C.c_void_p] * 3
+        L.polish_peaks_with_weights.restype = None
+        self.L = L
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_SO)
+
+    def peak_AB(self, refc, reft, n=None):
+        x_lo, x_hi, dy0 = refc
+        n = reft["n"] if n is None else n
+        P = x_lo.shape[0]
+        A = np.empty((P, n)); B = np.empty((P, n))
+        self.L.compute_peak_AB(P, _p(x_lo), _p(x_hi), _p(dy0), n, _p(reft["alpha"]), _p(reft["gamma"]),
+                               _p(reft["ghi_lo"]), _p(reft["ghi_hi"]), _p(reft["glo_lo"]), _p(reft["glo_hi"]),
+                               _p(reft["psi_lo"]), _p(reft["psi_hi"]), _p(A), _p(B))
+        return A, B
+
+    def polish(self, A, B, gamma, w, half, steps):
+        P, n = A.shape
+        hu, hp, dp = np.empty(P), np.empty(P), np.empty(P)
+        self.L.polish_peaks_with_weights(P, n, _p(np.ascontiguousarray(A)), _p(np.ascontiguousarray(B)),
+                                         _p(np.ascontiguousarray(gamma[:n])), _p(np.ascontiguousarray(w[:n])),
+                                         float(half), int(steps), _p(hu), _p(hp), _p(dp))
+        return hu, hp, dp

@@ -1,0 +1,68 @@
+"""The oracle itself: exact phase against Python integers, binary128 sums against the
+reference's own compiled evaluator (oracle/_ref), and against the committed golden vectors."""
+import numpy as np
+import pytest
+
+from mertens_bound_b200 import synth
+from oracle.oracle import RefLib, phase128_bigint, reference_candidates, reference_format
+
+MASK64 = (1 << 64) - 1
+
+
+def test_phase_c_matches_bigint(oracle, small_table):
+    cd = synth.make_candidates(6, seed=11)
+    # edge candidates: all-ones limbs, zero fraction, maximal integer part
+    extra = synth.Candidates(np.array([MASK64, 0, 3_600_000_000_000_000_000], dtype=np.uint64),
+                             np.array([MASK64, 0, 1], dtype=np.uint64), np.zeros(3))
+    for c in (cd, extra):
+        hi, lo = oracle.phase128(c, small_table.G3[:300])
+        for p in range(c.n):
+            for j in range(0, 300, 7):
+                h, l = phase128_bigint(c.v_int[p], c.v_frac[p], small_table.G3[j])
+                assert (int(hi[p, j]), int(lo[p, j])) == (h, l)
+
+
+def test_phase_edge_limbs(oracle):
+    G3 = np.array([[0, 0, 0], [0xFFFFFFFF, MASK64, MASK64], [1, 1 << 63, 1], [123456, MASK64, 0]], dtype=np.uint64)
+    c = synth.Candidates(np.array([MASK64, 1, 0], dtype=np.uint64), np.array([MASK64, MASK64, 1], dtype=np.uint64), np.zeros(3))
+    hi, lo = oracle.phase128(c, G3)
+    for p in range(3):
+        for j in range(4):
+            assert (int(hi[p, j]), int(lo[p, j])) == phase128_bigint(c.v_int[p], c.v_frac[p], G3[j])
+
+
+@pytest.mark.skipif(not RefLib.available(), reason="reference evaluator not built")
+def test_quad_oracle_matches_reference_evaluator(oracle, small_table):
+    """K2 from the reference's compute_peak_AB + h0 (path1_eval_fast.cpp:15-53, :76-81) on the
+    same table in the reference layout agrees with the binary128 oracle to FP64 rounding."""
+    t = small_table.truncate(3000)
+    cd = synth.make_candidates(16, seed=12)
+    k = 3e-9
+    hi, _ = oracle.k2(cd, t, k, t.n)
+    R = RefLib()
+    A, B = R.peak_AB(reference_candidates(cd), reference_format(t))
+    w = np.exp(-k * t.gamma ** 2)
+    h0, _, _ = R.polish(A, B, t.gamma, w, 2.5e-4, 0)
+    assert np.max(np.abs(h0 - hi[:, 0])) < 5e-14
+    dd = -(B @ (w * t.gamma))
+    dk = -(A @ (w * t.gamma ** 2))
+    assert np.max(np.abs(dd - hi[:, 1])) < 1e-14 * np.max(np.abs(hi[:, 1])) * 100
+    assert np.max(np.abs(dk - hi[:, 2])) < 1e-14 * np.max(np.abs(hi[:, 2])) * 100
+
+
+@pytest.mark.skipif(not RefLib.available(), reason="reference evaluator not built")
+def test_reference_phase_reduction_restated(oracle, small_table):
+    """path1_eval_fast.cpp:45-46 with dy0 = 0 (fraction bits below 2^-34 zero) gives the exact
+    phase plus arg(c)/2pi in its top word, to within one unit of 2^-64."""
+    t = small_table.truncate(500)
+    cd = synth.make_candidates(4, seed=13)
+    cd.v_frac[:] = cd.v_frac & ~np.uint64((1 << 34) - 1)
+    reft = reference_format(t)
+    A, B, top = oracle.ref_peak_AB(reference_candidates(cd), reft, want_top=True)
+    hi, lo = oracle.phase128(cd, t.G3)
+    for p in range(cd.n):
+        for j in range(t.n):
+            psi = (int(reft["psi_hi"][j]) << 64) | int(reft["psi_lo"][j])
+            want = ((((int(hi[p, j]) << 64) | int(lo[p, j])) - psi) % (1 << 128)) >> 64
+            d = (int(top[p, j]) - want) % (1 << 64)
+            assert d in (0, 1, (1 << 64) - 1)
