@@ -81,6 +81,40 @@ int mb_k2_plain_dev(mb_table *t, int64_t P, const uint64_t *d_v_int, const uint6
                     const double *d_delta, double k, double T, double *d_val, double *d_dd,
                     double *d_dk, void *stream);
 
+/* ---- chosen form: batched, precision-tiered value + gradient ----------------------------
+ * A plan fixes n_groups groups; group g is the next counts[g] candidates of the candidate
+ * array, evaluated at (ks[g], Ts[g]).  Per group the zeros below T are split at a boundary
+ * n_heavy chosen so that the a-priori worst-case error bound stays <= tol: the first n_heavy
+ * zeros are summed in FP64 (64-bit phase, FP64 polynomials), the rest with a 32-bit phase,
+ * MUFU sine/cosine and FP32 accumulation with two-sum compensated partials.  All groups run
+ * in one persistent kernel; mb_plan_run replays a captured CUDA graph.
+ * Replaces the candidate scoring loops of search/eval_tech1_600k.py:201-273,
+ * search/eval_tech2_hdrop_600k.py:127-201 and search/eval_sub35_candidates.py:64-138 (which
+ * call compute_peak_AB + polish_peaks_with_weights per weight vector), and the k-scan of
+ * search/path1_kernel_opt.py:526,687. */
+typedef struct mb_plan mb_plan;
+
+int mb_plan_create(mb_table *t, int n_groups, const int64_t *counts, const double *ks,
+                   const double *Ts, double tol, mb_plan **out);
+int mb_plan_destroy(mb_plan *p);
+/* Override the tile shape of group g: cpt in {1,2,4} candidates per thread, nzw in {1,2,4,8}
+ * warps splitting the zeros, chunk sizes in zeros (0 = automatic; multiples of 128 / 256). */
+int mb_plan_set_shape(mb_plan *p, int g, int cpt, int nzw, int64_t heavy_chunk, int64_t light_chunk);
+int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, int *n_items);
+int mb_plan_group_info(const mb_plan *p, int g, int64_t *n_T, int64_t *n_heavy, double *err_bound,
+                       double *sum_abs);
+/* Device pointers (P = sum of counts), asynchronous on `stream`. */
+int mb_plan_run_dev(mb_plan *p, const uint64_t *d_v_int, const uint64_t *d_v_frac,
+                    const double *d_delta, double *d_val, double *d_dd, double *d_dk, void *stream);
+/* Host pointers: copies through pinned staging and replays the plan's CUDA graph
+ * (H2D, kernels, D2H); returns when the results are in val/dd/dk. */
+int mb_plan_run(mb_plan *p, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
+                double *val, double *dd, double *dk);
+/* One-group convenience: plan, run, destroy.  *err_bound receives the a-priori bound. */
+int mb_k2_fast(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+               const double *delta, double k, double T, double tol, double *out_val, double *out_dd,
+               double *out_dk, double *err_bound);
+
 #ifdef __cplusplus
 }
 #endif

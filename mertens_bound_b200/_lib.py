@@ -31,6 +31,14 @@ SIGNATURES: dict[str, tuple] = {
     "mb_phase128": (i32, [vp, i64, vp, vp, i64, vp, vp]),
     "mb_k2_plain": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp]),
     "mb_k2_plain_dev": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
+    "mb_plan_create": (i32, [vp, i32, vp, vp, vp, f64, C.POINTER(vp)]),
+    "mb_plan_destroy": (i32, [vp]),
+    "mb_plan_set_shape": (i32, [vp, i32, i32, i32, i64, i64]),
+    "mb_plan_info": (i32, [vp, i64p, f64p, C.POINTER(i32)]),
+    "mb_plan_group_info": (i32, [vp, i32, i64p, i64p, f64p, f64p]),
+    "mb_plan_run_dev": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
+    "mb_plan_run": (i32, [vp, vp, vp, vp, vp, vp, vp]),
+    "mb_k2_fast": (i32, [vp, i64, vp, vp, vp, f64, f64, f64, vp, vp, vp, f64p]),
 }
 
 

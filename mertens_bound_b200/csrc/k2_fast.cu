@@ -1,0 +1,388 @@
+// The chosen form: batched, precision-tiered K2 value + gradient.
+//
+// Each group (k, T, a range of candidates) splits its zeros [0, n_T) at a boundary n_h chosen
+// from an a-priori error bound (host, k2_plan.cu):
+//   heavy tier  j <  n_h : 64-bit phase (3 IMAD.lo + 8 DFMA, error ~2^-48 turn), quarter-turn
+//                          FP64 polynomials, FP64 accumulation.          -> k2_heavy_kernel
+//   light tier  j >= n_h : 32-bit phase (3 IMAD.lo + 4 DFMA), MUFU sin/cos of the reduced
+//                          phase, FP32 accumulation flushed every LIGHT_FLUSH terms by two-sum
+//                          into float-float partials.                    -> k2_light_kernel
+// The heavy kernel is persistent with one CTA per SM (FP64-pipe bound); the light kernel is
+// launched concurrently on a second stream with one CTA per work item and fills the rest of
+// each SM (XU / FMA / integer pipes), so the two tiers overlap on every SM.
+//
+// Phase algebra (v = a1 2^32 + a0 + (d1 2^-32 + d0 2^-64), G = gI + b1 2^-32 + b0 2^-64 +
+// c1 2^-96 + c0 2^-128, all limbs 32-bit):
+//   frac(vG) 2^32 = [a1 b0 + a0 b1 + d1 gI]                       (exact mod 2^32, IMAD.lo)
+//                 + (a0 b0 + a1 c1 + d0 gI + d1 b1) 2^-32           (< 2^34, FP64)
+//                 + (a1 c0 + a0 c1 + d1 b0 + d0 b1) 2^-64 + ...     (< 4 units)
+// The FP64 sum is formed on top of 1.5 2^52, so each DFMA rounds it to an integer and the low
+// mantissa word holds it mod 2^32 (error <= 2 units of 2^-32 turn).
+// arg(c)/2pi (psi) is added to the phase, so each term is a cos(2pi u) with a = 2|c| w.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "k2_common.cuh"
+#include "k2_fast.h"
+#include "k2_internal.h"
+
+namespace mb {
+
+constexpr double MAGIC = 6755399441055744.0;   // 1.5 2^52
+constexpr double TWO_M32 = 2.3283064365386963e-10;
+constexpr double TWO_M64 = 5.421010862427522e-20;
+constexpr double TWO_M96 = 1.2621774483536189e-29;
+
+struct __align__(16) ZLight {   // 64 B
+    uint32_t b0, b1, gi, psi32;  // psi32 = round(psi 2^32) + 2 (centres the truncation bias)
+    double b0s, c1s, gis, b1s;   // limb 2^-32 (exact)
+    float a, b, d, pad;          // a = 2|c|w, b = -a gamma, d = -a gamma^2
+};
+
+struct __align__(16) ZHeavy {   // 112 B
+    uint32_t b0, b1, gi, pad;
+    double b0s, c1s, gis, b1s;   // limb 2^-64
+    double c0t, c1t, b0t, b1t;   // limb 2^-96
+    double psi;                  // arg(c)/2pi in turns
+    double a, b, d;
+};
+
+constexpr int FAST_THREADS = 256;
+constexpr int LIGHT_TILE = 256;
+constexpr int HEAVY_TILE = 128;
+constexpr int LIGHT_FLUSH = 16;
+// shared memory: the staged tile, reused after the tile loop for the cross-warp reduction
+constexpr int FAST_SMEM = 24576;
+static_assert(FAST_SMEM >= LIGHT_TILE * sizeof(ZLight), "light tile");
+static_assert(FAST_SMEM >= HEAVY_TILE * sizeof(ZHeavy), "heavy tile");
+static_assert(FAST_SMEM >= FAST_THREADS * 4 * 3 * sizeof(double), "reduction buffer");
+
+// Candidate registers shared by both tiers.
+struct CandRegs {
+    uint32_t a0, a1, d1;
+    double A0, A1, D0, D1;      // exact doubles of the limbs a0, a1, d0, d1
+};
+
+MB_DEV CandRegs cand_regs(const CandView &c, int64_t p, bool valid) {
+    Cand64 v{0, 0};
+    if (valid) v = fold_delta(c.vi[p], c.vf[p], c.delta ? c.delta[p] : 0.0);
+    CandRegs r;
+    r.a0 = (uint32_t)v.vi;
+    r.a1 = (uint32_t)(v.vi >> 32);
+    r.d1 = (uint32_t)(v.vf >> 32);
+    r.A0 = u32_to_f64(r.a0);
+    r.A1 = u32_to_f64(r.a1);
+    r.D0 = u32_to_f64((uint32_t)v.vf);
+    r.D1 = u32_to_f64(r.d1);
+    return r;
+}
+
+// Two-sum of floats: s + e = a + b exactly.
+MB_DEV void two_sum(float a, float b, float &s, float &e) {
+    s = a + b;
+    float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+template <int CPT>
+MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
+                       float (&hi)[CPT][3], float (&lo)[CPT][3]) {
+    float acc[CPT][3];
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
+    int cnt = 0;
+    for (int jj = zl; jj < nt; jj += ZL) {
+        const ZLight z = tile[jj];
+#pragma unroll
+        for (int i = 0; i < CPT; ++i) {
+            uint32_t lo32 = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi;
+            double R = fma(cr[i].A0, z.b0s, fma(cr[i].A1, z.c1s, fma(cr[i].D0, z.gis, fma(cr[i].D1, z.b1s, MAGIC))));
+            int32_t u = (int32_t)(lo32 + (uint32_t)__double2loint(R) + z.psi32);
+            float th = (float)u * 1.4629180792671596e-09f;      // 2pi 2^-32
+            float s = __sinf(th), co = __cosf(th);
+            acc[i][0] = fmaf(z.a, co, acc[i][0]);
+            acc[i][1] = fmaf(z.b, s, acc[i][1]);
+            acc[i][2] = fmaf(z.d, co, acc[i][2]);
+        }
+        if (++cnt == LIGHT_FLUSH) {
+            cnt = 0;
+#pragma unroll
+            for (int i = 0; i < CPT; ++i)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    float s, e;
+                    two_sum(hi[i][q], acc[i][q], s, e);
+                    hi[i][q] = s;
+                    lo[i][q] += e;
+                    acc[i][q] = 0.f;
+                }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < CPT; ++i)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            float s, e;
+            two_sum(hi[i][q], acc[i][q], s, e);
+            hi[i][q] = s;
+            lo[i][q] += e;
+        }
+}
+
+// sin/cos(2 pi y) for any y (turns) via quarter-turn reduction; FP64.
+MB_DEV void sincos_turns_quad(double y, double &sn, double &cs) {
+    double m = fma(y, 4.0, MAGIC);
+    int q = __double2loint(m);
+    double r = fma(-0.25, m - MAGIC, y);          // |r| <= 1/8 (exact)
+    double u = r * r;
+    double ps = QUAD_S[5];
+#pragma unroll
+    for (int k = 4; k >= 0; --k) ps = fma(ps, u, QUAD_S[k]);
+    double pc = QUAD_C[5];
+#pragma unroll
+    for (int k = 4; k >= 0; --k) pc = fma(pc, u, QUAD_C[k]);
+    double s = r * ps;
+    // rotate by q quarter turns: q=0 (s,c) 1 (c,-s) 2 (-s,-c) 3 (-c,s)
+    double S = (q & 1) ? pc : s;
+    double Cc = (q & 1) ? s : pc;
+    int sgn_s = (q & 2) << 30;
+    int sgn_c = ((q ^ (q >> 1)) & 1) << 31;
+    sn = __hiloint2double(__double2hiint(S) ^ sgn_s, __double2loint(S));
+    cs = __hiloint2double(__double2hiint(Cc) ^ sgn_c, __double2loint(Cc));
+}
+
+template <int CPT>
+MB_DEV void heavy_tile(const ZHeavy *tile, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
+                       double (&acc)[CPT][3]) {
+    for (int jj = zl; jj < nt; jj += ZL) {
+        const ZHeavy z = tile[jj];
+#pragma unroll
+        for (int i = 0; i < CPT; ++i) {
+            uint32_t lo32 = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi;
+            double F = fma(cr[i].A0, z.b0s, fma(cr[i].A1, z.c1s, fma(cr[i].D0, z.gis,
+                       fma(cr[i].D1, z.b1s, fma(cr[i].A1, z.c0t, fma(cr[i].A0, z.c1t,
+                       fma(cr[i].D1, z.b0t, cr[i].D0 * z.b1t)))))));
+            double y = fma(u32_to_f64(lo32), TWO_M32, F) + z.psi;
+            double sn, cs;
+            sincos_turns_quad(y, sn, cs);
+            acc[i][0] = fma(z.a, cs, acc[i][0]);
+            acc[i][1] = fma(z.b, sn, acc[i][1]);
+            acc[i][2] = fma(z.d, cs, acc[i][2]);
+        }
+    }
+}
+
+// Stage one zero into a tile record (one thread per zero).
+MB_DEV void stage_light(const TabView &t, int64_t j, double k, ZLight &r) {
+    double g = t.gamma[j];
+    double a = 2.0 * t.alpha[j] * exp(-k * g * g);
+    uint32_t b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j], c1 = t.g1[j];
+    r.b0 = b0; r.b1 = b1; r.gi = gi;
+    r.psi32 = (uint32_t)((t.psi[j] + 0x80000000ull) >> 32) + 2u;
+    r.b0s = u32_to_f64(b0) * TWO_M32;
+    r.c1s = u32_to_f64(c1) * TWO_M32;
+    r.gis = u32_to_f64(gi) * TWO_M32;
+    r.b1s = u32_to_f64(b1) * TWO_M32;
+    r.a = (float)a;
+    r.b = (float)(-a * g);
+    r.d = (float)(-a * g * g);
+    r.pad = 0.f;
+}
+
+MB_DEV void stage_heavy(const TabView &t, int64_t j, double k, ZHeavy &r) {
+    double g = t.gamma[j];
+    double a = 2.0 * t.alpha[j] * exp(-k * g * g);
+    uint32_t c0 = t.g0[j], c1 = t.g1[j], b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j];
+    r.b0 = b0; r.b1 = b1; r.gi = gi; r.pad = 0;
+    r.b0s = u32_to_f64(b0) * TWO_M64;
+    r.c1s = u32_to_f64(c1) * TWO_M64;
+    r.gis = u32_to_f64(gi) * TWO_M64;
+    r.b1s = u32_to_f64(b1) * TWO_M64;
+    r.c0t = u32_to_f64(c0) * TWO_M96;
+    r.c1t = u32_to_f64(c1) * TWO_M96;
+    r.b0t = u32_to_f64(b0) * TWO_M96;
+    r.b1t = u32_to_f64(b1) * TWO_M96;
+    uint64_t ps = t.psi[j];
+    r.psi = fma(u32_to_f64((uint32_t)(ps >> 32)), TWO_M32, u32_to_f64((uint32_t)ps) * TWO_M64);
+    r.a = a;
+    r.b = -a * g;
+    r.d = -a * g * g;
+}
+
+// Sum res over the nzw warps that share a candidate set, then warp zw==0 writes the partials.
+template <int CPT>
+MB_DEV void finish_item(const FastItem &it, const FastGroup &gr, double (&res)[CPT][3], int warp, int lane,
+                        int zw, int64_t cbase, int64_t cend, double *partial, unsigned char *smem) {
+    const int nzw = it.nzw;
+    __syncthreads();
+    double *red = reinterpret_cast<double *>(smem);
+    if (nzw > 1) {
+#pragma unroll
+        for (int i = 0; i < CPT; ++i)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) red[((warp * 32 + lane) * CPT + i) * 3 + q] = res[i][q];
+        __syncthreads();
+        if (zw == 0)
+            for (int w2 = 1; w2 < nzw; ++w2)
+#pragma unroll
+                for (int i = 0; i < CPT; ++i)
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) res[i][q] += red[(((warp + w2) * 32 + lane) * CPT + i) * 3 + q];
+    }
+    if (zw == 0) {
+#pragma unroll
+        for (int i = 0; i < CPT; ++i) {
+            int64_t p = cbase + i;
+            if (p < cend) {
+                double *o = partial + it.pbase + (p - gr.c0) * 3;
+                o[0] = res[i][0]; o[1] = res[i][1]; o[2] = res[i][2];
+            }
+        }
+    }
+}
+
+template <int CPT>
+MB_DEV void light_item(const FastItem &it, const FastGroup &gr, const TabView &t, const CandView &c,
+                       double *partial, unsigned char *smem) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nzw = it.nzw;
+    const int cgroup = warp / nzw, zw = warp - cgroup * nzw;
+    const int64_t cbase = it.c0 + (int64_t)(cgroup * 32 + lane) * CPT;
+    const int64_t cend = it.c0 + it.nc;
+    CandRegs cr[CPT];
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) cr[i] = cand_regs(c, cbase + i, cbase + i < cend);
+    ZLight *tile = reinterpret_cast<ZLight *>(smem);
+    float hi[CPT][3], lo[CPT][3];
+#pragma unroll
+    for (int i = 0; i < CPT; ++i)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) hi[i][q] = lo[i][q] = 0.f;
+    for (int64_t tb = it.z0; tb < it.z1; tb += LIGHT_TILE) {
+        __syncthreads();
+        int64_t j = tb + threadIdx.x;
+        if (threadIdx.x < LIGHT_TILE && j < it.z1) stage_light(t, j, gr.k, tile[threadIdx.x]);
+        __syncthreads();
+        light_tile<CPT>(tile, (int)min((int64_t)LIGHT_TILE, it.z1 - tb), zw, nzw, cr, hi, lo);
+    }
+    double res[CPT][3];
+#pragma unroll
+    for (int i = 0; i < CPT; ++i)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) res[i][q] = (double)hi[i][q] + (double)lo[i][q];
+    finish_item<CPT>(it, gr, res, warp, lane, zw, cbase, cend, partial, smem);
+}
+
+template <int CPT>
+MB_DEV void heavy_item(const FastItem &it, const FastGroup &gr, const TabView &t, const CandView &c,
+                       double *partial, unsigned char *smem) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nzw = it.nzw;
+    const int cgroup = warp / nzw, zw = warp - cgroup * nzw;
+    const int64_t cbase = it.c0 + (int64_t)(cgroup * 32 + lane) * CPT;
+    const int64_t cend = it.c0 + it.nc;
+    CandRegs cr[CPT];
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) cr[i] = cand_regs(c, cbase + i, cbase + i < cend);
+    ZHeavy *tile = reinterpret_cast<ZHeavy *>(smem);
+    double res[CPT][3];
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) res[i][0] = res[i][1] = res[i][2] = 0.0;
+    for (int64_t tb = it.z0; tb < it.z1; tb += HEAVY_TILE) {
+        __syncthreads();
+        int64_t j = tb + threadIdx.x;
+        if (threadIdx.x < HEAVY_TILE && j < it.z1) stage_heavy(t, j, gr.k, tile[threadIdx.x]);
+        __syncthreads();
+        heavy_tile<CPT>(tile, (int)min((int64_t)HEAVY_TILE, it.z1 - tb), zw, nzw, cr, res);
+    }
+    finish_item<CPT>(it, gr, res, warp, lane, zw, cbase, cend, partial, smem);
+}
+
+// Heavy tier: persistent, items pulled from an atomic counter (largest first).  At most 128
+// registers, so one heavy CTA leaves half of the SM's registers to light CTAs beside it.
+__global__ void __launch_bounds__(FAST_THREADS, 2)
+k2_heavy_kernel(TabView t, CandView c, const FastItem *items, int n_items, const FastGroup *groups,
+                int *counter, double *partial) {
+    __shared__ __align__(16) unsigned char smem[FAST_SMEM];
+    __shared__ int s_item;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int idx = s_item;
+        if (idx >= n_items) break;
+        const FastItem it = items[idx];
+        heavy_item<HEAVY_CPT>(it, groups[it.group], t, c, partial, smem);
+    }
+}
+
+// Light tier: one CTA per item.  MINB sets the register budget (65536 / (256 MINB)).
+template <int CPT, int MINB>
+__global__ void __launch_bounds__(FAST_THREADS, MINB)
+k2_light_kernel(TabView t, CandView c, const FastItem *items, const FastGroup *groups, double *partial) {
+    __shared__ __align__(16) unsigned char smem[FAST_SMEM];
+    const FastItem it = items[blockIdx.x];
+    light_item<CPT>(it, groups[it.group], t, c, partial, smem);
+}
+
+// Per candidate: sum the partials of its group's chunks in chunk order (deterministic).
+__global__ void fast_reduce_kernel(const FastGroup *groups, int n_groups, const double *partial,
+                                   int64_t P, double *val, double *dd, double *dk) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int g = 0;
+    while (g + 1 < n_groups && groups[g + 1].c0 <= p) ++g;
+    const FastGroup gr = groups[g];
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int ch = 0; ch < gr.n_chunks; ++ch) {
+        const double *o = partial + gr.pbase + ((int64_t)ch * gr.nc + (p - gr.c0)) * 3;
+        s0 += o[0]; s1 += o[1]; s2 += o[2];
+    }
+    val[p] = s0;
+    dd[p] = s1;
+    dk[p] = s2;
+}
+
+static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cudaStream_t s) {
+    if (pd.n_light == 0) return MB_OK;
+    dim3 grid((unsigned)pd.n_light);
+    const FastItem *li = pd.items + pd.n_heavy;
+    switch (pd.light_cpt) {
+        case 2: k2_light_kernel<2, 4><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+        case 3: k2_light_kernel<3, 3><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+        default: k2_light_kernel<4, 2><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+    }
+    MB_CUDA(cudaGetLastError());
+    return MB_OK;
+}
+
+int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
+                double *d_dk, cudaStream_t s) {
+    const TabView tv = view(t);
+    if (pd.n_heavy > 0) {
+        // fork: heavy tier on the table's side stream, concurrently with the light tier on s
+        MB_CUDA(cudaEventRecord(t.ev_fork, s));
+        MB_CUDA(cudaStreamWaitEvent(t.side, t.ev_fork, 0));
+        MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), t.side));
+        k2_heavy_kernel<<<pd.heavy_grid, FAST_THREADS, 0, t.side>>>(tv, c, pd.items, pd.n_heavy, pd.groups,
+                                                                    pd.counter, pd.partial);
+        MB_CUDA(cudaGetLastError());
+        MB_CUDA(cudaEventRecord(t.ev_join, t.side));
+    }
+    MB_TRY(launch_light(tv, pd, c, s));
+    if (pd.n_heavy > 0) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
+    fast_reduce_kernel<<<(unsigned)((c.P + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
+                                                                     d_val, d_dd, d_dk);
+    MB_CUDA(cudaGetLastError());
+    return MB_OK;
+}
+
+int heavy_grid_size(int device, unsigned *grid) {
+    int sms = 148;
+    MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    *grid = (unsigned)sms;   // one CTA per SM leaves room for light CTAs beside it
+    return MB_OK;
+}
+
+}  // namespace mb

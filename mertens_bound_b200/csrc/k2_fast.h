@@ -1,0 +1,60 @@
+// Work description of the chosen-form kernel (shared by k2_fast.cu and k2_plan.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "k2_internal.h"
+
+namespace mb {
+
+// One group: a contiguous candidate range evaluated at one (k, T).
+struct FastGroup {
+    int64_t c0, nc;    // candidates [c0, c0 + nc)
+    double k;
+    int64_t pbase;     // offset (in doubles) of this group's partial sums
+    int n_chunks;      // zero chunks (heavy then light); partial[pbase + (chunk*nc + p-c0)*3 + q]
+    int pad;
+};
+
+// One work item: a candidate tile of one group against one zero chunk of one tier.
+struct FastItem {
+    int64_t c0;        // first candidate (global index)
+    int64_t z0, z1;    // zeros [z0, z1)
+    int64_t pbase;     // group.pbase + chunk * group.nc * 3
+    int nc;            // candidates in this tile
+    int group;
+    int tier;          // 0 heavy (FP64), 1 light (FP32 + MUFU)
+    int cpt;           // candidates per thread: 1, 2 or 4
+    int nzw;           // warps splitting the zeros of one candidate set: 1..8
+    int pad;
+};
+
+constexpr int HEAVY_CPT = 4;     // candidates per thread in the heavy kernel
+
+// Device side of a plan: items[0, n_heavy) are heavy-tier items (pulled by the persistent
+// heavy kernel), items[n_heavy, n_heavy + n_light) light-tier items (one CTA each).
+struct FastPlanDev {
+    FastItem *items = nullptr;
+    FastGroup *groups = nullptr;
+    int n_heavy = 0, n_light = 0, n_groups = 0;
+    int light_cpt = 4;          // candidates per thread of the light kernel: 2, 3 or 4
+    unsigned heavy_grid = 0;
+    int *counter = nullptr;
+    double *partial = nullptr;
+};
+
+// Per-term worst-case absolute error of cos/sin (times amplitude) in each tier, per unit of
+// amplitude a_j = 2|c_j| w_j:
+//   light: MUFU sin/cos 2^-21.41 + argument roundings (int->float 2^-26 turn, 2pi scaling and
+//          the radians->turns product inside sin.approx, <= 2^-23 pi each) + phase 4.5 2^-32
+//          turn + amplitude and FFMA roundings (2 2^-24) + FP32 summation over a 16-term flush
+//          window (15 2^-24)  ->  2.2e-6
+//   heavy: phase 2^-47 turn, polynomial 5.6e-14, FP64 roundings  ->  2e-13
+constexpr double EPS_LIGHT = 2.2e-6;
+constexpr double EPS_HEAVY = 2.0e-13;
+
+int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
+                double *d_dk, cudaStream_t s);
+int heavy_grid_size(int device, unsigned *grid);
+
+}  // namespace mb

@@ -62,6 +62,8 @@ struct Table {
     std::vector<double> h_gamma;      // host copies for cutoffs and error planning
     std::vector<double> h_alpha;
     cudaStream_t stream = nullptr;    // the library's own stream for host-pointer calls
+    cudaStream_t side = nullptr;      // second stream: heavy tier beside the light tier
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // grow-only scratch owned by the table: `io` stages candidates and results of host-pointer
     // calls, `work` holds per-chunk partial sums.  Calls on one table must not overlap on the GPU.
     DevBuf io, work;

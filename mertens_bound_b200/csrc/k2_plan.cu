@@ -1,0 +1,364 @@
+// Plans for the chosen-form kernel: tier boundaries from an a-priori error bound, candidate
+// tiles and zero chunks as work items (largest first), partial-sum layout, and a CUDA graph
+// for repeated runs on fixed buffers.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "k2_fast.h"
+#include "k2_internal.h"
+
+using namespace mb;
+
+struct mb_plan {
+    Table *table = nullptr;
+    int n_groups = 0;
+    int64_t P = 0;
+    double tol = 1e-10;
+    std::vector<int64_t> counts;
+    std::vector<double> ks, Ts;
+    std::vector<FastGroup> groups;
+    std::vector<FastItem> items;
+    std::vector<int64_t> n_T, n_heavy;
+    std::vector<double> err_bound, sum_abs;
+    std::vector<int> shape_nzw;
+    std::vector<int64_t> heavy_chunk, light_chunk;
+    int light_cpt = 4;
+    int n_heavy_items = 0;
+    double zero_terms = 0;
+    FastPlanDev dev;
+    size_t partial_doubles = 0;
+    // host-pointer runs: device candidate/result buffers, pinned staging and a captured graph
+    uint64_t *d_vi = nullptr, *d_vf = nullptr;
+    double *d_delta = nullptr, *d_out = nullptr;
+    void *h_pinned = nullptr;
+    cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+void free_dev(mb_plan *p) {
+    cudaFree(p->dev.items);
+    cudaFree(p->dev.groups);
+    cudaFree(p->dev.counter);
+    cudaFree(p->dev.partial);
+    p->dev = FastPlanDev();
+}
+
+void free_io(mb_plan *p) {
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    p->graph = nullptr;
+    cudaFree(p->d_vi);
+    cudaFree(p->d_vf);
+    cudaFree(p->d_delta);
+    cudaFree(p->d_out);
+    if (p->h_pinned) cudaFreeHost(p->h_pinned);
+    p->d_vi = p->d_vf = nullptr;
+    p->d_delta = p->d_out = nullptr;
+    p->h_pinned = nullptr;
+}
+
+// Default number of warps splitting one candidate set's zeros, so that a candidate tile
+// ((8/nzw) * 32 * cpt candidates) is not much larger than the group.
+int default_nzw(int64_t P, int cpt) {
+    int nzw = 1;
+    while (nzw < 8 && (int64_t)(8 / nzw) * 32 * cpt > 2 * P) nzw *= 2;
+    return nzw;
+}
+
+// Tier boundary: the smallest n_h with EPS_LIGHT * sum_{j>=n_h} a_j <= budget, where
+// a_j = 2|c_j| exp(-k gamma_j^2) bounds |term_j|.  Returns the bound of the whole sum.
+void plan_tiers(const Table &t, int64_t n_use, double k, double tol, int64_t &n_h, double &bound,
+                double &sabs) {
+    std::vector<double> a(n_use);
+    double total = 0;
+    for (int64_t j = 0; j < n_use; ++j) {
+        double g = t.h_gamma[j];
+        a[j] = 2.0 * t.h_alpha[j] * std::exp(-k * g * g);
+        total += a[j];
+    }
+    const double budget = 0.5 * tol;
+    double tail = 0;
+    n_h = n_use;
+    for (int64_t j = n_use - 1; j >= 0; --j) {
+        if ((tail + a[j]) * EPS_LIGHT > budget) break;
+        tail += a[j];
+        n_h = j;
+    }
+    double heavy = total - tail;
+    // FP64 accumulation and reduction of the heavy sum and of the light partials: at most
+    // ~(terms per thread + chunks) roundings of 2^-53 relative; 1e-13 relative is a safe cover.
+    bound = EPS_LIGHT * tail + EPS_HEAVY * heavy + 1e-13 * total;
+    sabs = total;
+}
+
+// Work items.  Heavy items (FP64 tier) use HEAVY_CPT candidates per thread and are pulled by
+// the persistent heavy kernel (one CTA per SM); light items use the plan's light_cpt and run
+// one CTA each.  Chunk sizes aim at ~8 heavy items per heavy CTA and ~24 light items per SM.
+int build_items(mb_plan *p, int sms) {
+    p->groups.clear();
+    p->items.clear();
+    p->zero_terms = 0;
+    double Wh = 0, Wl = 0;
+    for (int g = 0; g < p->n_groups; ++g) {
+        Wh += (double)p->counts[g] * p->n_heavy[g];
+        Wl += (double)p->counts[g] * (p->n_T[g] - p->n_heavy[g]);
+    }
+    // ~4 items per heavy CTA (one per SM) and ~6 waves of light CTAs (about 3 per SM)
+    const double target_h = std::max(Wh / (4.0 * sms), 1.0);
+    const double target_l = std::max(Wl / (18.0 * sms), 1.0);
+    std::vector<FastItem> heavy, light;
+    int64_t c0 = 0, pbase = 0;
+    for (int g = 0; g < p->n_groups; ++g) {
+        FastGroup gr{};
+        gr.c0 = c0;
+        gr.nc = p->counts[g];
+        gr.k = p->ks[g];
+        gr.pbase = pbase;
+        const int nzw = p->shape_nzw[g];
+        const int64_t CTh = (int64_t)(8 / nzw) * 32 * HEAVY_CPT;
+        const int64_t CTl = (int64_t)(8 / nzw) * 32 * p->light_cpt;
+        int64_t hz = p->heavy_chunk[g], lz = p->light_chunk[g];
+        // chunk = target terms / tile candidates, rounded to whole tiles, at least 4 tiles
+        if (hz <= 0)
+            hz = std::max<int64_t>(512, ((int64_t)(target_h / std::min<int64_t>(CTh, std::max<int64_t>(gr.nc, 1))) + 64) / 128 * 128);
+        if (lz <= 0)
+            lz = std::max<int64_t>(1024, ((int64_t)(target_l / std::min<int64_t>(CTl, std::max<int64_t>(gr.nc, 1))) + 128) / 256 * 256);
+        int ch = 0;
+        auto emit = [&](int64_t z0, int64_t z1, int tier, int64_t CT, int cpt, std::vector<FastItem> &dst) {
+            for (int64_t ct = 0; ct * CT < gr.nc; ++ct) {
+                FastItem it{};
+                it.c0 = c0 + ct * CT;
+                it.nc = (int)std::min<int64_t>(CT, gr.nc - ct * CT);
+                it.group = g;
+                it.z0 = z0;
+                it.z1 = z1;
+                it.pbase = pbase + (int64_t)ch * gr.nc * 3;
+                it.tier = tier;
+                it.cpt = cpt;
+                it.nzw = nzw;
+                dst.push_back(it);
+            }
+            ++ch;
+        };
+        for (int64_t z = 0; z < p->n_heavy[g]; z += hz)
+            emit(z, std::min(z + hz, p->n_heavy[g]), 0, CTh, HEAVY_CPT, heavy);
+        for (int64_t z = p->n_heavy[g]; z < p->n_T[g]; z += lz)
+            emit(z, std::min(z + lz, p->n_T[g]), 1, CTl, p->light_cpt, light);
+        gr.n_chunks = ch;
+        p->zero_terms += (double)gr.nc * p->n_T[g];
+        pbase += (int64_t)gr.n_chunks * gr.nc * 3;
+        c0 += gr.nc;
+        p->groups.push_back(gr);
+    }
+    auto by_cost = [](const FastItem &a, const FastItem &b) {
+        return (double)a.nc * (a.z1 - a.z0) > (double)b.nc * (b.z1 - b.z0);
+    };
+    std::stable_sort(heavy.begin(), heavy.end(), by_cost);
+    std::stable_sort(light.begin(), light.end(), by_cost);
+    p->n_heavy_items = (int)heavy.size();
+    p->items = heavy;
+    p->items.insert(p->items.end(), light.begin(), light.end());
+    p->partial_doubles = (size_t)std::max<int64_t>(pbase, 3);
+    return MB_OK;
+}
+
+int upload(mb_plan *p) {
+    free_dev(p);
+    free_io(p);
+    int sms = 148;
+    MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->table->device));
+    MB_TRY(build_items(p, sms));
+    MB_CUDA(cudaMalloc(&p->dev.items, std::max<size_t>(1, p->items.size()) * sizeof(FastItem)));
+    MB_CUDA(cudaMalloc(&p->dev.groups, std::max<size_t>(1, p->groups.size()) * sizeof(FastGroup)));
+    MB_CUDA(cudaMalloc(&p->dev.counter, sizeof(int)));
+    MB_CUDA(cudaMalloc(&p->dev.partial, p->partial_doubles * sizeof(double)));
+    if (!p->items.empty())
+        MB_CUDA(cudaMemcpy(p->dev.items, p->items.data(), p->items.size() * sizeof(FastItem), cudaMemcpyHostToDevice));
+    MB_CUDA(cudaMemcpy(p->dev.groups, p->groups.data(), p->groups.size() * sizeof(FastGroup), cudaMemcpyHostToDevice));
+    p->dev.n_heavy = p->n_heavy_items;
+    p->dev.n_light = (int)p->items.size() - p->n_heavy_items;
+    p->dev.n_groups = (int)p->groups.size();
+    p->dev.light_cpt = p->light_cpt;
+    unsigned hg = 148;
+    MB_TRY(heavy_grid_size(p->table->device, &hg));
+    p->dev.heavy_grid = std::min<unsigned>(hg, (unsigned)std::max(1, p->n_heavy_items));
+    return MB_OK;
+}
+
+int plan_run_dev(mb_plan *p, const uint64_t *vi, const uint64_t *vf, const double *delta, double *val,
+                 double *dd, double *dk, cudaStream_t s) {
+    return launch_fast(*p->table, p->dev, CandView{vi, vf, delta, p->P}, val, dd, dk, s);
+}
+
+int ensure_io(mb_plan *p) {
+    if (p->d_out) return MB_OK;
+    size_t P = (size_t)std::max<int64_t>(p->P, 1);
+    MB_CUDA(cudaMalloc(&p->d_vi, P * 8));
+    MB_CUDA(cudaMalloc(&p->d_vf, P * 8));
+    MB_CUDA(cudaMalloc(&p->d_delta, P * 8));
+    MB_CUDA(cudaMalloc(&p->d_out, 3 * P * 8));
+    MB_CUDA(cudaHostAlloc(&p->h_pinned, 6 * P * 8, cudaHostAllocDefault));
+    // capture: H2D of the candidates, the kernels, D2H of the results
+    cudaStream_t s = p->table->stream;
+    char *h = (char *)p->h_pinned;
+    MB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(p->d_vi, h, P * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(p->d_vf, h + P * 8, P * 8, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(p->d_delta, h + 2 * P * 8, P * 8, cudaMemcpyHostToDevice, s);
+    int st = plan_run_dev(p, p->d_vi, p->d_vf, p->d_delta, p->d_out, p->d_out + P, p->d_out + 2 * P, s);
+    cudaMemcpyAsync(h + 3 * P * 8, p->d_out, 3 * P * 8, cudaMemcpyDeviceToHost, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (st != MB_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) {
+        set_error("plan graph capture: %s", cudaGetErrorString(e));
+        return MB_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&p->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        set_error("plan graph instantiate: %s", cudaGetErrorString(e));
+        return MB_ERR_CUDA;
+    }
+    return MB_OK;
+}
+
+}  // namespace
+
+extern "C" int mb_plan_create(mb_table *h, int n_groups, const int64_t *counts, const double *ks,
+                              const double *Ts, double tol, mb_plan **out) {
+    MB_CHECK_ARG(out != nullptr, "mb_plan_create: out is null");
+    *out = nullptr;
+    MB_CHECK_ARG(h && counts && ks && Ts, "mb_plan_create: null argument");
+    MB_CHECK_ARG(n_groups >= 1 && n_groups <= 4096, "mb_plan_create: n_groups=%d", n_groups);
+    MB_CHECK_ARG(std::isfinite(tol) && tol > 0, "mb_plan_create: tol=%g must be > 0", tol);
+    Table &t = table_of(h);
+    int64_t P = 0;
+    for (int g = 0; g < n_groups; ++g) {
+        MB_CHECK_ARG(counts[g] >= 0 && counts[g] <= ((int64_t)1 << 26), "mb_plan_create: count[%d]", g);
+        MB_CHECK_ARG(std::isfinite(ks[g]) && ks[g] >= 0, "mb_plan_create: k[%d]=%g", g, ks[g]);
+        MB_CHECK_ARG(!std::isnan(Ts[g]), "mb_plan_create: T[%d] is NaN", g);
+        P += counts[g];
+    }
+    MB_CHECK_ARG(P <= ((int64_t)1 << 26), "mb_plan_create: total P=%lld too large", (long long)P);
+    MB_TRY(device_guard(t.device));
+    mb_plan *p = new mb_plan();
+    p->table = &t;
+    p->n_groups = n_groups;
+    p->P = P;
+    p->tol = tol;
+    p->counts.assign(counts, counts + n_groups);
+    p->ks.assign(ks, ks + n_groups);
+    p->Ts.assign(Ts, Ts + n_groups);
+    p->n_T.resize(n_groups);
+    p->n_heavy.resize(n_groups);
+    p->err_bound.resize(n_groups);
+    p->sum_abs.resize(n_groups);
+    p->shape_nzw.resize(n_groups);
+    p->heavy_chunk.assign(n_groups, 0);
+    p->light_chunk.assign(n_groups, 0);
+    for (int g = 0; g < n_groups; ++g) {
+        p->n_T[g] = t.count_below(Ts[g]);
+        plan_tiers(t, p->n_T[g], ks[g], tol, p->n_heavy[g], p->err_bound[g], p->sum_abs[g]);
+        p->shape_nzw[g] = default_nzw(counts[g], p->light_cpt);
+    }
+    int st = upload(p);
+    if (st != MB_OK) {
+        free_dev(p);
+        delete p;
+        return st;
+    }
+    *out = p;
+    return MB_OK;
+}
+
+extern "C" int mb_plan_destroy(mb_plan *p) {
+    if (!p) return MB_OK;
+    device_guard(p->table->device);
+    free_io(p);
+    free_dev(p);
+    delete p;
+    return MB_OK;
+}
+
+extern "C" int mb_plan_set_shape(mb_plan *p, int g, int cpt, int nzw, int64_t heavy_chunk,
+                                 int64_t light_chunk) {
+    MB_CHECK_ARG(p && g >= 0 && g < p->n_groups, "mb_plan_set_shape: bad plan/group");
+    MB_CHECK_ARG(cpt == 2 || cpt == 3 || cpt == 4, "mb_plan_set_shape: light cpt=%d (2, 3 or 4)", cpt);
+    MB_CHECK_ARG(nzw == 1 || nzw == 2 || nzw == 4 || nzw == 8, "mb_plan_set_shape: nzw=%d", nzw);
+    MB_CHECK_ARG(heavy_chunk == 0 || (heavy_chunk > 0 && heavy_chunk % 128 == 0), "mb_plan_set_shape: heavy_chunk");
+    MB_CHECK_ARG(light_chunk == 0 || (light_chunk > 0 && light_chunk % 256 == 0), "mb_plan_set_shape: light_chunk");
+    p->light_cpt = cpt;    // plan-wide: the light kernel is instantiated per candidates-per-thread
+    p->shape_nzw[g] = nzw;
+    p->heavy_chunk[g] = heavy_chunk;
+    p->light_chunk[g] = light_chunk;
+    MB_TRY(device_guard(p->table->device));
+    return upload(p);
+}
+
+extern "C" int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, int *n_items) {
+    MB_CHECK_ARG(p, "mb_plan_info: null plan");
+    if (P) *P = p->P;
+    if (zero_terms) *zero_terms = p->zero_terms;
+    if (n_items) *n_items = (int)p->items.size();
+    return MB_OK;
+}
+
+extern "C" int mb_plan_group_info(const mb_plan *p, int g, int64_t *n_T, int64_t *n_heavy,
+                                  double *err_bound, double *sum_abs) {
+    MB_CHECK_ARG(p && g >= 0 && g < p->n_groups, "mb_plan_group_info: bad plan/group");
+    if (n_T) *n_T = p->n_T[g];
+    if (n_heavy) *n_heavy = p->n_heavy[g];
+    if (err_bound) *err_bound = p->err_bound[g];
+    if (sum_abs) *sum_abs = p->sum_abs[g];
+    return MB_OK;
+}
+
+extern "C" int mb_plan_run_dev(mb_plan *p, const uint64_t *d_vi, const uint64_t *d_vf,
+                               const double *d_delta, double *d_val, double *d_dd, double *d_dk,
+                               void *stream) {
+    MB_CHECK_ARG(p && d_vi && d_vf && d_val && d_dd && d_dk, "mb_plan_run_dev: null argument");
+    MB_TRY(device_guard(p->table->device));
+    return plan_run_dev(p, d_vi, d_vf, d_delta, d_val, d_dd, d_dk, (cudaStream_t)stream);
+}
+
+extern "C" int mb_plan_run(mb_plan *p, const uint64_t *vi, const uint64_t *vf, const double *delta,
+                           double *val, double *dd, double *dk) {
+    MB_CHECK_ARG(p && vi && vf && val, "mb_plan_run: null argument");
+    MB_TRY(device_guard(p->table->device));
+    if (p->P == 0) return MB_OK;
+    if (delta)
+        for (int64_t i = 0; i < p->P; ++i)
+            MB_CHECK_ARG(std::isfinite(delta[i]) && std::fabs(delta[i]) < 4.0e18, "mb_plan_run: delta[%lld]", (long long)i);
+    MB_TRY(ensure_io(p));
+    size_t P = (size_t)p->P;
+    char *h = (char *)p->h_pinned;
+    std::memcpy(h, vi, P * 8);
+    std::memcpy(h + P * 8, vf, P * 8);
+    if (delta) std::memcpy(h + 2 * P * 8, delta, P * 8);
+    else std::memset(h + 2 * P * 8, 0, P * 8);
+    MB_CUDA(cudaGraphLaunch(p->graph, p->table->stream));
+    MB_CUDA(cudaStreamSynchronize(p->table->stream));
+    const double *o = (const double *)(h + 3 * P * 8);
+    std::memcpy(val, o, P * 8);
+    if (dd) std::memcpy(dd, o + P, P * 8);
+    if (dk) std::memcpy(dk, o + 2 * P, P * 8);
+    return MB_OK;
+}
+
+extern "C" int mb_k2_fast(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                          const double *delta, double k, double T, double tol, double *out_val,
+                          double *out_dd, double *out_dk, double *err_bound) {
+    MB_CHECK_ARG(h && v_int && v_frac && out_val, "mb_k2_fast: null argument");
+    mb_plan *p = nullptr;
+    MB_TRY(mb_plan_create(h, 1, &P, &k, &T, tol, &p));
+    int st = mb_plan_run(p, v_int, v_frac, delta, out_val, out_dd, out_dk);
+    if (st == MB_OK && err_bound) *err_bound = p->err_bound[0];
+    mb_plan_destroy(p);
+    return st;
+}

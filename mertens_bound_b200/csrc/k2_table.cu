@@ -80,6 +80,9 @@ static void free_table(Table &t) {
     cudaFree(t.d_psi);
     t.io.release();
     t.work.release();
+    if (t.ev_fork) cudaEventDestroy(t.ev_fork);
+    if (t.ev_join) cudaEventDestroy(t.ev_join);
+    if (t.side) cudaStreamDestroy(t.side);
     if (t.stream) cudaStreamDestroy(t.stream);
     t = Table();
 }
@@ -175,7 +178,10 @@ extern "C" int mb_table_create(const uint64_t *G3, const double *c_re, const dou
     ALLOC_COPY(t.d_alpha, t.h_alpha.data(), n * sizeof(double));
     ALLOC_COPY(t.d_psi, psi.data(), n * sizeof(uint64_t));
 #undef ALLOC_COPY
-    if ((e = cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    if ((e = cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&t.side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&t.ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&t.ev_join, cudaEventDisableTiming)) != cudaSuccess) {
         set_error("mb_table_create: %s", cudaGetErrorString(e));
         return fail(MB_ERR_CUDA);
     }

@@ -105,3 +105,85 @@ def k2_plain(table: ZeroTable, cands, k: float, T: float = math.inf):
     check(_lib.lib().mb_k2_plain(table.handle, P, ptr(vi), ptr(vf), ptr(d), float(k), float(T),
                                  ptr(val), ptr(dd), ptr(dk)))
     return val, dd, dk
+
+
+class Plan:
+    """A batched evaluation plan: groups of candidates, each at its own (k, T).
+
+    counts[g] consecutive candidates form group g.  tol is the a-priori bound on |K2 error|
+    per candidate that fixes each group's heavy/light tier boundary.
+    """
+
+    def __init__(self, table: ZeroTable, counts, ks, Ts, tol: float = 1e-10):
+        counts = np.ascontiguousarray(counts, dtype=np.int64)
+        ks = np.ascontiguousarray(ks, dtype=np.float64)
+        Ts = np.ascontiguousarray(Ts, dtype=np.float64)
+        if not (counts.shape == ks.shape == Ts.shape) or counts.ndim != 1:
+            raise ValueError("counts, ks, Ts must be 1-D of equal length")
+        h = C.c_void_p()
+        check(_lib.lib().mb_plan_create(table.handle, counts.shape[0], ptr(counts), ptr(ks), ptr(Ts),
+                                        float(tol), C.byref(h)))
+        self._h = h
+        self.table = table
+        self.counts, self.ks, self.Ts, self.tol = counts, ks, Ts, tol
+        self.P = int(counts.sum())
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise ValueError("plan is closed")
+        return self._h
+
+    def set_shape(self, g: int, cpt: int, nzw: int, heavy_chunk: int = 0, light_chunk: int = 0):
+        check(_lib.lib().mb_plan_set_shape(self.handle, g, cpt, nzw, heavy_chunk, light_chunk))
+
+    def info(self):
+        P, zt, ni = C.c_int64(), C.c_double(), C.c_int()
+        check(_lib.lib().mb_plan_info(self.handle, C.byref(P), C.byref(zt), C.byref(ni)))
+        return {"P": P.value, "zero_terms": zt.value, "n_items": ni.value}
+
+    def group_info(self, g: int):
+        nT, nh, eb, sa = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
+        check(_lib.lib().mb_plan_group_info(self.handle, g, C.byref(nT), C.byref(nh), C.byref(eb), C.byref(sa)))
+        return {"n_T": nT.value, "n_heavy": nh.value, "err_bound": eb.value, "sum_abs": sa.value}
+
+    def run(self, cands):
+        """Host arrays in, host arrays out (graph replay through pinned staging)."""
+        vi, vf, d = _cand_arrays(cands)
+        if vi.shape[0] != self.P:
+            raise ValueError(f"plan expects {self.P} candidates, got {vi.shape[0]}")
+        val, dd, dk = np.empty(self.P), np.empty(self.P), np.empty(self.P)
+        check(_lib.lib().mb_plan_run(self.handle, ptr(vi), ptr(vf), ptr(d), ptr(val), ptr(dd), ptr(dk)))
+        return val, dd, dk
+
+    def run_dev(self, d_vi: int, d_vf: int, d_delta, d_val: int, d_dd: int, d_dk: int, stream: int = 0):
+        """Device pointers (ints), asynchronous on `stream`."""
+        check(_lib.lib().mb_plan_run_dev(self.handle, d_vi, d_vf, d_delta, d_val, d_dd, d_dk, stream))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.lib().mb_plan_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def k2_fast(table: ZeroTable, cands, k: float, T: float = math.inf, tol: float = 1e-10):
+    """Chosen-form K2, dK2/ddelta, dK2/dk and the a-priori error bound (one group)."""
+    vi, vf, d = _cand_arrays(cands)
+    P = vi.shape[0]
+    val, dd, dk = np.empty(P), np.empty(P), np.empty(P)
+    eb = C.c_double()
+    check(_lib.lib().mb_k2_fast(table.handle, P, ptr(vi), ptr(vf), ptr(d), float(k), float(T), float(tol),
+                                ptr(val), ptr(dd), ptr(dk), C.byref(eb)))
+    return val, dd, dk, eb.value

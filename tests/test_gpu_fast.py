@@ -1,0 +1,84 @@
+"""Chosen form (tiered FP32/FP64 persistent kernel) against the oracle and the plain kernel."""
+import math
+
+import numpy as np
+import pytest
+
+from mertens_bound_b200 import k2, synth
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10   # |K2 error| target of the chosen form
+
+
+@pytest.fixture(scope="module")
+def table(gpu, small_table):
+    t = k2.ZeroTable.from_data(small_table)
+    yield t
+    t.close()
+
+
+@pytest.mark.parametrize("P", [1, 37, 64, 700, 1500])
+def test_fast_vs_oracle(table, small_table, oracle, P):
+    cd = synth.make_candidates(P, seed=100 + P)
+    k = 3e-9
+    val, dd, dk, eb = k2.k2_fast(table, cd, k, tol=TOL)
+    assert eb <= TOL
+    n = min(P, 64)
+    ohi, _ = oracle.k2(cd.subset(np.arange(n)), small_table, k, small_table.n)
+    err = np.abs(val[:n] - ohi[:, 0])
+    assert np.max(err) <= eb, (np.max(err), eb)
+    # gradients: same a-priori structure scaled by gamma; compare relative to their size
+    assert np.max(np.abs(dd[:n] - ohi[:, 1])) <= 1e-6 * np.max(np.abs(ohi[:, 1]))
+    assert np.max(np.abs(dk[:n] - ohi[:, 2])) <= 1e-6 * np.max(np.abs(ohi[:, 2]))
+
+
+def test_fast_matches_plain_with_delta_and_cutoff(table):
+    cd = synth.make_candidates(512, seed=7)
+    cd.delta[:] = np.random.default_rng(3).uniform(-2e-4, 2e-4, 512)
+    k, T = 1e-9, 20000.0
+    val, dd, dk, eb = k2.k2_fast(table, cd, k, T)
+    pv, pd, pk = k2.k2_plain(table, cd, k, T)
+    assert np.max(np.abs(val - pv)) <= eb
+    assert np.max(np.abs(dd - pd)) <= 1e-6 * np.max(np.abs(pd))
+
+
+def test_batched_plan_groups(table):
+    counts = [64, 300, 1024, 5]
+    ks = [3e-9, 1e-9, 1.5e-10, 3e-9]
+    Ts = [math.inf, 20000.0, 50000.0, 1000.0]
+    P = sum(counts)
+    cd = synth.make_candidates(P, seed=8)
+    with k2.Plan(table, counts, ks, Ts, tol=TOL) as plan:
+        val, dd, dk = plan.run(cd)
+        val2, _, _ = plan.run(cd)            # graph replay gives identical results
+        assert np.array_equal(val, val2)
+        off = 0
+        for g, (c, kk, TT) in enumerate(zip(counts, ks, Ts)):
+            sub = cd.subset(np.arange(off, off + c))
+            pv, pd, pk = k2.k2_plain(table, sub, kk, TT)
+            gi = plan.group_info(g)
+            assert gi["err_bound"] <= TOL
+            assert np.max(np.abs(val[off:off + c] - pv)) <= gi["err_bound"]
+            off += c
+
+
+def test_plan_shapes_agree(table):
+    cd = synth.make_candidates(256, seed=9)
+    with k2.Plan(table, [256], [3e-9], [math.inf]) as plan:
+        ref, _, _ = plan.run(cd)
+        eb = plan.group_info(0)["err_bound"]
+        for cpt, nzw in [(2, 1), (3, 2), (4, 8), (2, 8)]:
+            plan.set_shape(0, cpt, nzw, 256, 512)
+            v, _, _ = plan.run(cd)
+            assert np.max(np.abs(v - ref)) <= 2 * eb
+
+
+def test_all_heavy_when_tolerance_tight(table, small_table, oracle):
+    cd = synth.make_candidates(16, seed=10)
+    with k2.Plan(table, [16], [3e-9], [math.inf], tol=1e-14) as plan:
+        gi = plan.group_info(0)
+        assert gi["n_heavy"] == gi["n_T"]
+        val, _, _ = plan.run(cd)
+    ohi, _ = oracle.k2(cd, small_table, 3e-9, small_table.n)
+    assert np.max(np.abs(val - ohi[:, 0])) < 1e-12
