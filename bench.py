@@ -1,0 +1,344 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 K2 evaluator (one JSON line on rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (search-scoring shape): a synthetic table of all zeros below T0 = 3e5 (466,659
+zeros), 4,096 candidate points v ~ 3.5e18 per GPU, k = 3e-9.  One step = K2 value and both
+derivatives (dK2/ddelta, dK2/dk) for every candidate over every zero below T0, i.e.
+4,096 x 466,659 zero-terms, with |K2 error| bounded a priori by tol = 1e-10.
+
+Arms
+  ours       the chosen form (tiered, batched plan) timed on the device with CUDA events,
+             inputs resident in HBM; beside it the plain FP64 kernel (the ratio's denominator),
+             the end-to-end number through the host-pointer API (pinned H2D + graph + D2H),
+             a roofline of the dominant kernel, and the reference CPU evaluator timed on a
+             bounded sample (cpu_baseline).
+  reference  the reference's own CPU evaluator (search/path1_eval_fast.cpp compiled into
+             oracle/_ref) on the same workload and metric, a bounded candidate sample per step.
+
+Multi-GPU (torchrun): every rank evaluates its own 4,096 candidates over the same table
+(candidates shard with no data-path collective: weak scaling); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "K₂ zero-terms/s (value+grad, |err|≤1e-10 vs Arb): chosen form vs plain FP64, 1 B200"
+UNIT = "zero-terms/s"
+T0, K_GAUSS, P_PER_GPU, TOL = 3e5, 3e-9, 4096, 1e-10
+WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 candidates v~3.5e18 "
+            "per GPU, k=3e-9, K2 + dK2/ddelta + dK2/dk per candidate, a-priori |err| <= 1e-10")
+# Thread instructions per zero-term of the light-tier kernel (the dominant kernel), from the
+# ncu capture summarised in profiles/k2_light_kernel_search_scoring.md.
+LIGHT_INST_PER_TERM = 22.5
+REF_SAMPLE_CANDS = 64
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(prefix="mb_clocks_", suffix=".csv")
+        self.f = open(self.path, "w")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={CLOCK_QUERY}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------- reference CPU evaluator
+
+def reference_rate(table, cands, k: float, n_use: int, seconds: float, steps: int | None = None):
+    """Zero-terms/s of the reference's compute_peak_AB plus the value and gradient sums
+    (h0 = sum w A as in path1_eval_fast.cpp:76-81, dK2/dv = -sum w gamma B,
+    dK2/dk = -sum w gamma^2 A) on REF_SAMPLE_CANDS candidates per call."""
+    from oracle.oracle import Oracle, RefLib, reference_candidates, reference_format
+
+    reft = reference_format(table, n_use, exact_psi=False)
+    w = np.exp(-k * table.gamma[:n_use] ** 2)
+    wg, wg2 = w * table.gamma[:n_use], w * table.gamma[:n_use] ** 2
+    if RefLib.available():
+        R, kind, cores = RefLib(), "reference", 16           # team size fixed by the source (:33)
+        peak_ab = lambda refc: R.peak_AB(refc, reft)
+    else:
+        O, kind, cores = Oracle(), "port", 1
+        peak_ab = lambda refc: O.ref_peak_AB(refc, reft)
+    P = cands.n
+    done, t_total, calls = 0, 0.0, 0
+    idx = 0
+    while True:
+        sel = np.arange(idx, idx + REF_SAMPLE_CANDS) % P
+        idx += REF_SAMPLE_CANDS
+        refc = reference_candidates(cands.subset(sel))
+        t = time.perf_counter()
+        A, B = peak_ab(refc)
+        h0, dd, dk = A @ w, -(B @ wg), -(A @ wg2)
+        t_total += time.perf_counter() - t
+        done += REF_SAMPLE_CANDS * n_use
+        calls += 1
+        if (steps is not None and calls >= steps) or (steps is None and t_total >= seconds):
+            break
+    return done / t_total, kind, cores, calls, t_total
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from mertens_bound_b200 import k2, synth, _lib
+    from mertens_bound_b200._lib import check
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    data = synth.make_table_below(T0, seed=1)
+    cands = synth.make_candidates(P_PER_GPU, seed=3 + rank)
+    P = cands.n
+    table = k2.ZeroTable.from_data(data, device=local)
+    n_T = table.count_below(T0)
+    terms = float(P) * n_T
+
+    vi = torch.from_numpy(cands.v_int.view(np.int64)).to(dev)
+    vf = torch.from_numpy(cands.v_frac.view(np.int64)).to(dev)
+    dl = torch.zeros(P, dtype=torch.float64, device=dev)
+    out = torch.empty(3, P, dtype=torch.float64, device=dev)
+    ref = torch.empty(3, P, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)   # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    L = _lib.lib()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for s in range(steps):
+            flush.fill_(s & 0xFF)                # evict table + candidates from L2 between steps
+            ev[s][0].record(stream)
+            fn()
+            ev[s][1].record(stream)
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) for a, b in ev]
+
+    # plain FP64 kernel (denominator of the ratio)
+    def plain():
+        check(L.mb_k2_plain_dev(table.handle, P, vi.data_ptr(), vf.data_ptr(), dl.data_ptr(), K_GAUSS, T0,
+                                ref[0].data_ptr(), ref[1].data_ptr(), ref[2].data_ptr(), sptr))
+    plain_ms = timed(plain, max(3, args.steps // 10), 2)
+
+    plan = k2.Plan(table, [P], [K_GAUSS], [T0], tol=TOL)
+    gi = plan.group_info(0)
+
+    def fast(tiers=3):
+        check(L.mb_plan_run_tiers_dev(plan.handle, tiers, vi.data_ptr(), vf.data_ptr(), dl.data_ptr(),
+                                      out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), sptr))
+
+    # headline: chosen form, exactly K timed steps bracketed by barrier + synchronize
+    for _ in range(max(3, args.warmup)):
+        fast()
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(local)
+    t_wall = time.perf_counter()
+    step_ms = timed(fast, args.steps, 0)
+    barrier()
+    torch.cuda.synchronize(dev)
+    wall_s = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(sum(step_ms))
+    value = world * terms * args.steps / (total_ms * 1e-3)
+    ms_per_step = total_ms / args.steps
+    diff = (out - ref).abs().max(dim=1).values.cpu().numpy()
+
+    # per-tier kernels on their own (roofline of the dominant kernel)
+    light_ms = statistics.median(timed(lambda: fast(2), 5, 1))
+    heavy_ms = statistics.median(timed(lambda: fast(1), 5, 1))
+    ht, lt = C_double_pair(L.mb_plan_tier_terms, plan.handle)
+    peak = C_double(L.mb_calibrate_issue, local)
+    light_achieved = LIGHT_INST_PER_TERM * lt / (light_ms * 1e-3)
+
+    # end to end through the host-pointer API (pinned H2D, graph, D2H), every step
+    for _ in range(3):
+        plan.run(cands)
+    barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        plan.run(cands)
+    e2e_s = max_over_ranks(time.perf_counter() - t)
+    e2e_value = world * terms * args.steps / e2e_s
+
+    plain_rate = terms / (statistics.median(plain_ms) * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32 phase + f64 (heavy tier) + f32 (light tier)",
+        "data": "synthetic (seeded zero table and candidates; no real zeta zeros)",
+        "config": {"workload": WORKLOAD, "zeros": n_T, "candidates_per_gpu": P, "k": K_GAUSS, "T0": T0,
+                   "tol": TOL, "heavy_zeros": gi["n_heavy"], "err_bound": gi["err_bound"],
+                   "l2": "256 MB buffer written between timed steps (table 28 MB < L2)",
+                   "parallelism": f"candidates sharded over {world} GPU(s), no collective on the data path",
+                   "wall_s_timed_region": wall_s},
+        "plain_fp64": {"value": world * plain_rate, "ms_per_step": statistics.median(plain_ms)},
+        "speedup_vs_plain": world * plain_rate and value / (world * plain_rate),
+        "max_abs_diff_vs_plain": {"val": float(diff[0]), "dd": float(diff[1]), "dk": float(diff[2])},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * P, "d2h_bytes_per_step": 3 * 8 * P},
+        "roofline": {"bound": "issue", "kernel": "k2_light_kernel", "achieved": light_achieved / 1e12,
+                     "peak": peak / 1e12, "unit": "T thread-inst/s", "frac": light_achieved / peak,
+                     "traffic": None, "per_term_inst": LIGHT_INST_PER_TERM, "light_ms": light_ms,
+                     "heavy_ms": heavy_ms, "light_terms": lt, "heavy_terms": ht,
+                     "peak_source": "measured live: FFMA issue rate (mb_calibrate_issue); MEASURED_PEAKS.json "
+                                    "has only HBM and bf16-tensor peaks, neither binds this kernel"},
+        "clocks": clocks,
+        "gpu_launches": 3 * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, calls, secs = reference_rate(data, cands, K_GAUSS, n_T, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                "sample": f"{calls} calls x {REF_SAMPLE_CANDS} candidates x {n_T} zeros "
+                                          f"({secs:.1f} s): compute_peak_AB + value/grad sums",
+                                "nproc": os.cpu_count()}
+    plan.close()
+    table.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def C_double(fn, *args):
+    import ctypes as C
+    from mertens_bound_b200._lib import check
+    x = C.c_double()
+    check(fn(*args, C.byref(x)))
+    return x.value
+
+
+def C_double_pair(fn, *args):
+    import ctypes as C
+    from mertens_bound_b200._lib import check
+    a, b = C.c_double(), C.c_double()
+    check(fn(*args, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from mertens_bound_b200 import synth
+    data = synth.make_table_below(T0, seed=1)
+    cands = synth.make_candidates(P_PER_GPU, seed=3)
+    n_T = data.count_below(T0)
+    reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=max(1, args.warmup))     # warm-up
+    rate, kind, cores, calls, secs = reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=args.steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / calls * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (same table and candidates as the ours arm)",
+        "config": {"workload": WORKLOAD, "zeros": n_T, "candidates_per_step": REF_SAMPLE_CANDS},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{REF_SAMPLE_CANDS} candidates x {n_T} zeros per step",
+                         "nproc": os.cpu_count()},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

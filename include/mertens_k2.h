@@ -110,6 +110,16 @@ int mb_plan_run_dev(mb_plan *p, const uint64_t *d_v_int, const uint64_t *d_v_fra
  * (H2D, kernels, D2H); returns when the results are in val/dd/dk. */
 int mb_plan_run(mb_plan *p, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
                 double *val, double *dd, double *dk);
+/* Run one tier only (tiers: 1 heavy, 2 light, 3 both = mb_plan_run_dev), to time a kernel on
+ * its own; with 1 or 2 the results miss the other tier's terms.  No reference counterpart. */
+int mb_plan_run_tiers_dev(mb_plan *p, int tiers, const uint64_t *d_v_int, const uint64_t *d_v_frac,
+                          const double *d_delta, double *d_val, double *d_dd, double *d_dk, void *stream);
+/* Zero-terms per run in each tier. */
+int mb_plan_tier_terms(const mb_plan *p, double *heavy_terms, double *light_terms);
+/* Measured full-rate instruction issue throughput of `device` (FFMA chains), in thread
+ * instructions per second: the peak against which the ALU-bound kernels are reported. */
+int mb_calibrate_issue(int device, double *thread_inst_per_s);
+
 /* One-group convenience: plan, run, destroy.  *err_bound receives the a-priori bound. */
 int mb_k2_fast(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                const double *delta, double k, double T, double tol, double *out_val, double *out_dd,

@@ -66,7 +66,45 @@ def main():
         kind = "rel." if rel else "abs."
         out.append(f"// {name}: degree {deg} in u, max {kind} fit error {mp.nstr(err, 3)}")
         out.append(emit(name, c, ctype, fmt))
+    out += certified_sets()
     print("\n".join(out))
+
+
+def outward(q):
+    """Doubles (lo, hi) with lo <= q <= hi for an exact rational q."""
+    import math
+    from fractions import Fraction
+    d = float(q)
+    lo = d if Fraction(d) <= q else math.nextafter(d, -math.inf)
+    hi = d if Fraction(d) >= q else math.nextafter(d, math.inf)
+    return lo, hi
+
+
+def certified_sets():
+    """Taylor coefficients of sin x / x and cos x in u = x^2 as outward-rounded intervals
+    (exact rationals (-1)^k/(2k+1)! and (-1)^k/(2k)!), and an enclosure of pi/2, for the
+    directed-rounding interval kernel.  Used on 0 <= x <= pi/4 with the Lagrange remainder
+    x^19/19! (sine, 9 terms) and x^20/20! (cosine, 10 terms) added separately."""
+    import math
+    from fractions import Fraction
+    s = [Fraction((-1) ** k, math.factorial(2 * k + 1)) for k in range(9)]
+    c = [Fraction((-1) ** k, math.factorial(2 * k)) for k in range(10)]
+    out = ["// CERT_*: exact Taylor coefficients rounded outward (lo <= exact <= hi)"]
+    for name, q in (("CERT_S", s), ("CERT_C", c)):
+        lo, hi = zip(*(outward(x) for x in q))
+        out.append(f"static __device__ __constant__ const double {name}_LO[{len(q)}] = {{{', '.join(repr(x) for x in lo)}}};")
+        out.append(f"static __device__ __constant__ const double {name}_HI[{len(q)}] = {{{', '.join(repr(x) for x in hi)}}};")
+    with mp.workprec(300):
+        pio2 = mp.pi / 2
+        num, den = (pio2 * mp.mpf(2) ** 300), mp.mpf(2) ** 300
+        q = Fraction(int(mp.floor(num)), int(den))
+        lo, _ = outward(q)
+        _, hi = outward(q + Fraction(1, int(den)))
+    out.append(f"#define CERT_PIO2_LO {lo!r}")
+    out.append(f"#define CERT_PIO2_HI {hi!r}")
+    out.append(f"#define CERT_REM_S {outward(Fraction(1, math.factorial(19)))[1]!r}   // 1/19! rounded up")
+    out.append(f"#define CERT_REM_C {outward(Fraction(1, math.factorial(20)))[1]!r}   // 1/20! rounded up")
+    return out
 
 
 if __name__ == "__main__":

@@ -357,10 +357,14 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
     return MB_OK;
 }
 
+// tiers: bit 0 runs the heavy tier, bit 1 the light tier (3 = the full evaluation; a single
+// tier is used to time one kernel on its own -- the result then lacks the other tier).
 int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
-                double *d_dk, cudaStream_t s) {
+                double *d_dk, cudaStream_t s, int tiers) {
     const TabView tv = view(t);
-    if (pd.n_heavy > 0) {
+    const bool heavy = (tiers & 1) && pd.n_heavy > 0;
+    const bool light = (tiers & 2) && pd.n_light > 0;
+    if (heavy) {
         // fork: heavy tier on the table's side stream, concurrently with the light tier on s
         MB_CUDA(cudaEventRecord(t.ev_fork, s));
         MB_CUDA(cudaStreamWaitEvent(t.side, t.ev_fork, 0));
@@ -370,11 +374,60 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
         MB_CUDA(cudaGetLastError());
         MB_CUDA(cudaEventRecord(t.ev_join, t.side));
     }
-    MB_TRY(launch_light(tv, pd, c, s));
-    if (pd.n_heavy > 0) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
+    if (light) MB_TRY(launch_light(tv, pd, c, s));
+    if (heavy) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
     fast_reduce_kernel<<<(unsigned)((c.P + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
                                                                      d_val, d_dd, d_dk);
     MB_CUDA(cudaGetLastError());
+    return MB_OK;
+}
+
+// Issue-rate calibration: independent FFMA chains (full-rate instruction), 8 per thread.
+__global__ void __launch_bounds__(256) issue_calibration_kernel(int iters, float *sink) {
+    float f[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i] = 1.0f + 1e-3f * (threadIdx.x + i);
+    const float a = 0.99999994f, b = 1e-7f;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) asm volatile("fma.rn.f32 %0, %0, %1, %2;" : "+f"(f[i]) : "f"(a), "f"(b));
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += f[i];
+    if (s == 123.25f) sink[0] = s;
+}
+
+int calibrate_issue(int device, double *thread_inst_per_s) {
+    int sms = 148;
+    MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    float *sink = nullptr;
+    MB_CUDA(cudaMalloc(&sink, sizeof(float)));
+    cudaEvent_t e0, e1;
+    MB_CUDA(cudaEventCreate(&e0));
+    MB_CUDA(cudaEventCreate(&e1));
+    const int iters = 8192;
+    const unsigned grid = (unsigned)sms * 8;
+    issue_calibration_kernel<<<grid, 256>>>(64, sink);
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+        cudaEventRecord(e0);
+        issue_calibration_kernel<<<grid, 256>>>(iters, sink);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (e != cudaSuccess) {
+        set_error("calibration: %s", cudaGetErrorString(e));
+        return MB_ERR_CUDA;
+    }
+    *thread_inst_per_s = (double)grid * 256 * iters * 8 / (best * 1e-3);
     return MB_OK;
 }
 

@@ -54,7 +54,8 @@ constexpr double EPS_LIGHT = 2.2e-6;
 constexpr double EPS_HEAVY = 2.0e-13;
 
 int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
-                double *d_dk, cudaStream_t s);
+                double *d_dk, cudaStream_t s, int tiers = 3);
 int heavy_grid_size(int device, unsigned *grid);
+int calibrate_issue(int device, double *thread_inst_per_s);
 
 }  // namespace mb

@@ -327,6 +327,34 @@ extern "C" int mb_plan_run_dev(mb_plan *p, const uint64_t *d_vi, const uint64_t 
     return plan_run_dev(p, d_vi, d_vf, d_delta, d_val, d_dd, d_dk, (cudaStream_t)stream);
 }
 
+extern "C" int mb_plan_run_tiers_dev(mb_plan *p, int tiers, const uint64_t *d_vi, const uint64_t *d_vf,
+                                     const double *d_delta, double *d_val, double *d_dd, double *d_dk,
+                                     void *stream) {
+    MB_CHECK_ARG(p && d_vi && d_vf && d_val && d_dd && d_dk, "mb_plan_run_tiers_dev: null argument");
+    MB_CHECK_ARG(tiers >= 1 && tiers <= 3, "mb_plan_run_tiers_dev: tiers=%d (1 heavy, 2 light, 3 both)", tiers);
+    MB_TRY(device_guard(p->table->device));
+    return launch_fast(*p->table, p->dev, CandView{d_vi, d_vf, d_delta, p->P}, d_val, d_dd, d_dk,
+                       (cudaStream_t)stream, tiers);
+}
+
+extern "C" int mb_plan_tier_terms(const mb_plan *p, double *heavy_terms, double *light_terms) {
+    MB_CHECK_ARG(p, "mb_plan_tier_terms: null plan");
+    double h = 0, l = 0;
+    for (int g = 0; g < p->n_groups; ++g) {
+        h += (double)p->counts[g] * p->n_heavy[g];
+        l += (double)p->counts[g] * (p->n_T[g] - p->n_heavy[g]);
+    }
+    if (heavy_terms) *heavy_terms = h;
+    if (light_terms) *light_terms = l;
+    return MB_OK;
+}
+
+extern "C" int mb_calibrate_issue(int device, double *thread_inst_per_s) {
+    MB_CHECK_ARG(thread_inst_per_s, "mb_calibrate_issue: null output");
+    MB_TRY(device_guard(device));
+    return calibrate_issue(device, thread_inst_per_s);
+}
+
 extern "C" int mb_plan_run(mb_plan *p, const uint64_t *vi, const uint64_t *vf, const double *delta,
                            double *val, double *dd, double *dk) {
     MB_CHECK_ARG(p && vi && vf && val, "mb_plan_run: null argument");

@@ -131,25 +131,46 @@ def _rint_shift(x: int, s: int) -> int:
     return q
 
 
-def reference_format(table, n=None):
-    """The table in the reference's zeros_600k.bin field set (planar arrays)."""
-    import mpmath as mp
+def reference_format(table, n=None, exact_psi=True):
+    """The table in the reference's zeros_600k.bin field set (planar arrays).
 
+    ghi = G 2^146 mod 2^128 and glo = rint(G 2^98) (round half to even) are exact integer
+    transforms of the 64.128 fixed-point G, done limb-wise in numpy.  psi is computed from
+    the FP64 c at 256 bits with mpmath (exact_psi) or in FP64 (top 53 bits only)."""
     n = table.G3.shape[0] if n is None else n
-    out = {k: np.empty(n, dtype=np.uint64) for k in ("ghi_lo", "ghi_hi", "glo_lo", "glo_hi", "psi_lo", "psi_hi")}
-    with mp.workprec(256):
-        two_pi = 2 * mp.pi
-        for j in range(n):
-            gi, g1, g2 = (int(x) for x in table.G3[j])
-            Gf = (gi << 128) | (g1 << 64) | g2
-            ghi = (Gf << 18) & MASK128                 # G 2^146 mod 2^128 (exact)
-            glo = _rint_shift(Gf, 30) & MASK128        # rint(G 2^98)
-            a = mp.atan2(mp.mpf(float(table.c_im[j])), mp.mpf(float(table.c_re[j])))
-            frac = (-a / two_pi) % 1
-            psi = int(mp.nint(frac * mp.mpf(2) ** 128)) & MASK128
-            out["ghi_lo"][j], out["ghi_hi"][j] = ghi & MASK64, ghi >> 64
-            out["glo_lo"][j], out["glo_hi"][j] = glo & MASK64, glo >> 64
-            out["psi_lo"][j], out["psi_hi"][j] = psi & MASK64, psi >> 64
+    G3 = np.ascontiguousarray(table.G3[:n], dtype=np.uint64)
+    gi, g1, g2 = G3[:, 0], G3[:, 1], G3[:, 2]
+    u = np.uint64
+    out = {}
+    # G 2^146 mod 2^128 = (g1 2^64 + g2) 2^18 mod 2^128
+    out["ghi_hi"] = (g1 << u(18)) | (g2 >> u(46))
+    out["ghi_lo"] = g2 << u(18)
+    # G 2^98 = Gfix / 2^30 with Gfix = gi 2^128 + g1 2^64 + g2, rounded half to even
+    hi = (gi << u(34)) | (g1 >> u(30))
+    lo = (g1 << u(34)) | (g2 >> u(30))
+    rem = g2 & u((1 << 30) - 1)
+    half = u(1 << 29)
+    up = (rem > half) | ((rem == half) & ((lo & u(1)) == u(1)))
+    lo2 = lo + up.astype(np.uint64)
+    hi = hi + ((lo2 < lo) & up).astype(np.uint64)
+    out["glo_hi"], out["glo_lo"] = hi, lo2
+    if exact_psi:
+        import mpmath as mp
+        out["psi_lo"] = np.empty(n, dtype=np.uint64)
+        out["psi_hi"] = np.empty(n, dtype=np.uint64)
+        with mp.workprec(256):
+            two_pi = 2 * mp.pi
+            for j in range(n):
+                a = mp.atan2(mp.mpf(float(table.c_im[j])), mp.mpf(float(table.c_re[j])))
+                psi = int(mp.nint(((-a / two_pi) % 1) * mp.mpf(2) ** 128)) & MASK128
+                out["psi_lo"][j], out["psi_hi"][j] = psi & MASK64, psi >> 64
+    else:
+        f = np.mod(-np.arctan2(table.c_im[:n], table.c_re[:n]) / (2 * np.pi), 1.0)
+        s = np.minimum(f * 2.0**64, np.nextafter(2.0**64, 0))
+        out["psi_hi"] = s.astype(np.uint64)
+        out["psi_lo"] = np.zeros(n, dtype=np.uint64)
+    for key in ("ghi_lo", "ghi_hi", "glo_lo", "glo_hi", "psi_lo", "psi_hi"):
+        out[key] = np.ascontiguousarray(out[key])
     out["alpha"] = np.ascontiguousarray(np.hypot(table.c_re[:n], table.c_im[:n]))
     out["gamma"] = np.ascontiguousarray(table.gamma[:n])
     out["n"] = n
