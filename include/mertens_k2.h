@@ -81,6 +81,22 @@ int mb_k2_plain_dev(mb_table *t, int64_t P, const uint64_t *d_v_int, const uint6
                     const double *d_delta, double k, double T, double *d_val, double *d_dd,
                     double *d_dk, void *stream);
 
+/* Plain FP64 K2 for callers that cannot allocate device memory: no counterpart in the
+ * reference (its evaluator is host code).  Callers in a host callback, inside a fixed memory
+ * budget or in a runtime that owns every allocation cannot call cudaMalloc; this entry point
+ * allocates nothing.  The caller passes the zero data as device arrays in the library's
+ * layout -- d_g = five planar u32 limb arrays of G 2^128 (least significant first, stride
+ * n_zeros), d_gamma, d_cre, d_cim -- sums the first n_use zeros, and passes candidates and
+ * outputs as device arrays.  Scratch for the partial sums is a fixed 8 MiB device array that
+ * every GPU loading the library keeps until exit, so P <= 349,525 (larger P returns
+ * MB_ERR_CAPACITY).  Calls that overlap on the GPU race on that array.  The first call on a
+ * device looks up the array's address; make it before any stream capture.
+ * Runs on the current device, asynchronously on `stream`. */
+int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamma, const double *d_cre,
+                            const double *d_cim, int64_t n_zeros, int64_t n_use, int64_t P,
+                            const uint64_t *d_v_int, const uint64_t *d_v_frac, const double *d_delta,
+                            double k, double *d_val, double *d_dd, double *d_dk, void *stream);
+
 /* ---- chosen form: batched, precision-tiered value + gradient ----------------------------
  * A plan fixes n_groups groups; group g is the next counts[g] candidates of the candidate
  * array, evaluated at (ks[g], Ts[g]).  Per group the zeros below T are split at a boundary

@@ -6,6 +6,7 @@
 // reduction inside the CTA and a deterministic FP64 reduction across zero chunks.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "k2_common.cuh"
 #include "k2_internal.h"
@@ -236,3 +237,108 @@ int launch_plain(Table &t, CandView c, int64_t n_use, double k, double *d_val, d
 }
 
 }  // namespace mb
+
+// ------------------------------------------------------------------ no-allocation entry point
+//
+// For callers that cannot allocate device memory themselves: code running where cudaMalloc is
+// not allowed or not wanted (inside a host callback, a real-time or pre-reserved memory budget,
+// an embedding runtime that owns all allocations).  The per-chunk partial sums of the plain
+// kernel go to a fixed file-scope device array instead of a table-owned buffer, and the zero
+// data and candidates are passed as plain device pointers, so a call allocates nothing.
+//
+// The array holds NOALLOC_PARTIAL_DOUBLES doubles (8 MiB); every GPU that loads this library
+// keeps it until the process exits.  P is limited to NOALLOC_PARTIAL_DOUBLES / 3 candidates.
+// All calls on a device share the array: calls that overlap on the GPU (different streams,
+// host threads) race on it.  A call overwrites every slot it later reads, so no earlier
+// contents leak into a result.  The first call on a device looks up the array's device
+// address (cudaGetSymbolAddress); make that first call before any stream capture.
+namespace {
+
+constexpr int64_t NOALLOC_PARTIAL_DOUBLES = (int64_t)1 << 20;
+static __device__ __align__(256) double g_noalloc_partial[NOALLOC_PARTIAL_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+std::mutex g_noalloc_mu;
+
+// Device address of the array on the current device (set up once per device).
+int noalloc_scratch(double **out) {
+    int dev = -1;
+    MB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        mb::set_error("no-allocation scratch: device %d out of range", dev);
+        return MB_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        double *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_partial);
+        if (e != cudaSuccess || p == nullptr) {
+            mb::set_error("cudaGetSymbolAddress for the no-allocation scratch failed: %s",
+                          cudaGetErrorString(e));
+            return MB_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return MB_OK;
+}
+
+}  // namespace
+
+extern "C" int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamma, const double *d_cre,
+                                       const double *d_cim, int64_t n_zeros, int64_t n_use, int64_t P,
+                                       const uint64_t *d_v_int, const uint64_t *d_v_frac,
+                                       const double *d_delta, double k, double *d_val, double *d_dd,
+                                       double *d_dk, void *stream) {
+    using namespace mb;
+    MB_CHECK_ARG(P >= 0 && P * 3 <= NOALLOC_PARTIAL_DOUBLES,
+                 "mb_k2_plain_noalloc_dev: P=%lld exceeds the fixed scratch (at most %lld candidates)",
+                 (long long)P, (long long)(NOALLOC_PARTIAL_DOUBLES / 3));
+    MB_CHECK_ARG(d_g && d_gamma && d_cre && d_cim && d_v_int && d_v_frac && d_val && d_dd && d_dk,
+                 "mb_k2_plain_noalloc_dev: null argument");
+    MB_CHECK_ARG(n_zeros >= 1 && n_use >= 0 && n_use <= n_zeros, "mb_k2_plain_noalloc_dev: n_use=%lld n_zeros=%lld",
+                 (long long)n_use, (long long)n_zeros);
+    MB_CHECK_ARG(std::isfinite(k) && k >= 0.0, "mb_k2_plain_noalloc_dev: k=%g", k);
+    if (P == 0) return MB_OK;
+    double *partial = nullptr;
+    MB_TRY(noalloc_scratch(&partial));
+    int dev = 0;
+    MB_CUDA(cudaGetDevice(&dev));
+    cudaStream_t s = (cudaStream_t)stream;
+    TabView tv{};
+    tv.g0 = d_g;
+    tv.g1 = d_g + n_zeros;
+    tv.g2 = d_g + 2 * n_zeros;
+    tv.g3 = d_g + 3 * n_zeros;
+    tv.g4 = d_g + 4 * n_zeros;
+    tv.gamma = d_gamma;
+    tv.cre = d_cre;
+    tv.cim = d_cim;
+    tv.n = n_zeros;
+    CandView c{d_v_int, d_v_frac, d_delta, P};
+    PlainShape sh = plain_shape(P);
+    int64_t cta_c = sh.cands_per_cta();
+    int64_t n_ctile = (P + cta_c - 1) / cta_c;
+    int64_t n_chunk = std::max<int64_t>(1, ((int64_t)sm_count(dev) * 8 + n_ctile - 1) / n_ctile);
+    n_chunk = std::min(n_chunk, std::max<int64_t>(1, (n_use + PLAIN_TILE - 1) / PLAIN_TILE));
+    n_chunk = std::min(n_chunk, NOALLOC_PARTIAL_DOUBLES / (3 * P));      // fits the fixed array
+    int64_t chunk = std::max<int64_t>(1, (n_use + n_chunk - 1) / n_chunk);
+    chunk = ((chunk + PLAIN_TILE - 1) / PLAIN_TILE) * PLAIN_TILE;
+    n_chunk = std::max<int64_t>(1, (n_use + chunk - 1) / chunk);
+    if (n_use == 0) {
+        // nothing to sum: clear the one chunk the reduction reads
+        MB_CUDA(cudaMemsetAsync(partial, 0, (size_t)P * 3 * sizeof(double), s));
+        n_chunk = 1;
+    } else {
+        dim3 grid((unsigned)n_ctile, (unsigned)n_chunk);
+        if (sh.cpt == 2)
+            k2_plain_kernel<2><<<grid, PLAIN_THREADS, 0, s>>>(tv, c, n_use, chunk, k, sh.lpc_log2, sh.nzw, partial);
+        else
+            k2_plain_kernel<1><<<grid, PLAIN_THREADS, 0, s>>>(tv, c, n_use, chunk, k, sh.lpc_log2, sh.nzw, partial);
+        MB_CUDA(cudaGetLastError());
+    }
+    reduce_partials_kernel<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(partial, P, (int)n_chunk, d_val, d_dd, d_dk);
+    MB_CUDA(cudaGetLastError());
+    return MB_OK;
+}
