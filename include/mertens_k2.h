@@ -81,6 +81,17 @@ int mb_k2_plain_dev(mb_table *t, int64_t P, const uint64_t *d_v_int, const uint6
                     const double *d_delta, double k, double T, double *d_val, double *d_dd,
                     double *d_dk, void *stream);
 
+/* Certified interval: out_lo[p] <= K2 <= out_hi[p] rigorously (directed rounding, Taylor
+ * enclosures of sine/cosine with Lagrange remainders, CUDA exp() within 2 ulp) for the
+ * table's exact G and c, v = v_int + v_frac 2^-64 widened by v_rad[p] (nullable) and each
+ * term widened by 2 w term_rad[j] (nullable; n = count_below(T) entries, e.g. the radius of
+ * c e^{i gamma v} implied by the input balls).  out_abs_hi (nullable) bounds sum 2 w |c|.
+ * P <= 65535.  Replaces the ball sum of certification/certify_K2.py:100-133 (work) over all
+ * batches and its serial reduction :179-192. */
+int mb_k2_certified(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                    const double *v_rad, double k, double T, const double *term_rad, double *out_lo,
+                    double *out_hi, double *out_abs_hi);
+
 /* Plain FP64 K2 for callers that cannot allocate device memory: no counterpart in the
  * reference (its evaluator is host code).  Callers in a host callback, inside a fixed memory
  * budget or in a runtime that owns every allocation cannot call cudaMalloc; this entry point

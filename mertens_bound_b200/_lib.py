@@ -43,6 +43,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_plan_tier_terms": (i32, [vp, f64p, f64p]),
     "mb_calibrate_issue": (i32, [i32, f64p]),
     "mb_k2_plain_noalloc_dev": (i32, [vp, vp, vp, vp, i64, i64, i64, vp, vp, vp, f64, vp, vp, vp, vp]),
+    "mb_k2_certified": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
 }
 
 

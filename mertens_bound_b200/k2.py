@@ -178,6 +178,24 @@ class Plan:
             pass
 
 
+def k2_certified(table: ZeroTable, cands, k: float, T: float = math.inf, v_rad=None, term_rad=None):
+    """Rigorous enclosure [lo, hi] of K2 at v = v_int + v_frac 2^-64 (delta must be zero or
+    absent; widen with v_rad instead), plus an upper bound of sum 2 w |c|."""
+    vi, vf, d = _cand_arrays(cands)
+    if d is not None and np.any(d != 0):
+        raise ValueError("the certified evaluation takes exact 64.64 points; pass offsets as v_rad")
+    P = vi.shape[0]
+    vr = None if v_rad is None else _f64(np.broadcast_to(v_rad, (P,)))
+    n_use = table.count_below(T)
+    tr = None if term_rad is None else _f64(term_rad)
+    if tr is not None and tr.shape != (n_use,):
+        raise ValueError(f"term_rad must have count_below(T) = {n_use} entries")
+    lo, hi, ab = np.empty(P), np.empty(P), np.empty(P)
+    check(_lib.lib().mb_k2_certified(table.handle, P, ptr(vi), ptr(vf), ptr(vr), float(k), float(T), ptr(tr),
+                                     ptr(lo), ptr(hi), ptr(ab)))
+    return lo, hi, ab
+
+
 def k2_fast(table: ZeroTable, cands, k: float, T: float = math.inf, tol: float = 1e-10):
     """Chosen-form K2, dK2/ddelta, dK2/dk and the a-priori error bound (one group)."""
     vi, vf, d = _cand_arrays(cands)

@@ -53,6 +53,16 @@ def k2_ball(vi: int, vf: int, delta: float, G3, c_re, c_im, k: float, n_use: int
             iv.prec = old
 
 
+def _exact(t) -> Fraction:
+    """Exact value of an mpmath raw float tuple (sign, mantissa, exponent, bitcount)."""
+    sign, man, e, _ = t
+    if man == 0 and e != 0:
+        raise ValueError("non-finite interval endpoint")
+    v = Fraction(man) * Fraction(2) ** e
+    return -v if sign else v
+
+
 def bounds(x) -> tuple[Fraction, Fraction]:
-    """Exact rational endpoints of an mpmath interval."""
-    return Fraction(*mp.mpf(x.a).as_integer_ratio()), Fraction(*mp.mpf(x.b).as_integer_ratio())
+    """Exact rational endpoints of an mpmath interval (read without rounding)."""
+    a, b = x._mpi_
+    return _exact(a), _exact(b)

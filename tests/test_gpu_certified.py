@@ -1,0 +1,72 @@
+"""Certified interval kernel: its [lo, hi] must contain the interval oracle's ball (mpmath iv,
+the restatement of certify_K2.py's Arb sum) and the binary128 value."""
+import math
+import time
+
+import numpy as np
+import pytest
+
+from mertens_bound_b200 import k2, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def table(gpu, small_table):
+    t = k2.ZeroTable.from_data(small_table)
+    yield t
+    t.close()
+
+
+def test_certified_contains_interval_ball(table, small_table):
+    from oracle.interval import bounds, k2_ball
+    n = 1200
+    cd = synth.make_candidates(3, seed=51)
+    T = float(small_table.gamma[n - 1]) + 1e-9
+    assert table.count_below(T) == n
+    lo, hi, ab = k2.k2_certified(table, cd, 3e-9, T)
+    for p in range(cd.n):
+        val, _, _ = k2_ball(cd.v_int[p], cd.v_frac[p], 0.0, small_table.G3, small_table.c_re, small_table.c_im,
+                            3e-9, n)
+        blo, bhi = bounds(val)
+        assert lo[p] <= blo and bhi <= hi[p], (lo[p], float(blo), float(bhi), hi[p])
+        assert hi[p] - lo[p] < 1e-12
+
+
+def test_certified_contains_quad_oracle(table, small_table, oracle):
+    cd = synth.make_candidates(40, seed=52)
+    for k, T in ((3e-9, math.inf), (1e-9, 20000.0), (0.0, 3000.0)):
+        lo, hi, ab = k2.k2_certified(table, cd, k, T)
+        ohi, olo = oracle.k2(cd, small_table, k, small_table.count_below(T))
+        v = ohi[:, 0] + olo[:, 0]
+        assert np.all(lo <= v) and np.all(v <= hi)
+        assert np.max(hi - lo) < 1e-11
+        assert np.all(ab >= np.abs(lo)) and np.all(ab >= np.abs(hi))
+
+
+def test_certified_radii_widen(table):
+    cd = synth.make_candidates(2, seed=53)
+    lo0, hi0, _ = k2.k2_certified(table, cd, 3e-9)
+    lo1, hi1, _ = k2.k2_certified(table, cd, 3e-9, v_rad=1e-12)
+    assert np.all(lo1 <= lo0) and np.all(hi1 >= hi0) and np.all(hi1 - lo1 > hi0 - lo0)
+    rad = np.full(table.n, 1e-9)
+    lo2, hi2, _ = k2.k2_certified(table, cd, 3e-9, term_rad=rad)
+    assert np.all(hi2 - lo2 > 1e-9)
+
+
+def test_certified_full_peak2(gpu, oracle):
+    """All 2,325,572 zeros below T0 = 1.3e6 at the reference's Peak2 point
+    (certification/certify_K2.py:40-43), k = 1.5e-10, in well under a second."""
+    data = synth.make_table(2_325_572, seed=1)
+    cd = synth.peak2_candidate()
+    with k2.ZeroTable.from_data(data) as t:
+        assert t.count_below(1.3e6) == 2_325_572
+        k2.k2_certified(t, cd, 1.5e-10, 1.3e6)                       # warm-up
+        t0 = time.perf_counter()
+        lo, hi, ab = k2.k2_certified(t, cd, 1.5e-10, 1.3e6, v_rad=2.0 ** -64)
+        elapsed = time.perf_counter() - t0
+    assert elapsed < 1.0
+    ohi, olo = oracle.k2(cd, data, 1.5e-10, data.n)
+    v = ohi[0, 0] + olo[0, 0]
+    assert lo[0] <= v <= hi[0]
+    assert hi[0] - lo[0] < 1e-11

@@ -31,6 +31,26 @@ def test_phase_edge_limbs(oracle):
             assert (int(hi[p, j]), int(lo[p, j])) == phase128_bigint(c.v_int[p], c.v_frac[p], G3[j])
 
 
+def test_interval_ball_contains_quad(oracle, small_table):
+    """The mpmath interval restatement of the Arb sum encloses the binary128 value and is
+    far narrower than the 1e-10 bar."""
+    from fractions import Fraction
+    from oracle.interval import bounds, k2_ball
+    n = 300
+    cd = synth.make_candidates(2, seed=14)
+    cd.delta[:] = [0.0, 3e-5]
+    hi, lo = oracle.k2(cd, small_table, 3e-9, n)
+    for p in range(2):
+        val, dd, dk = k2_ball(cd.v_int[p], cd.v_frac[p], cd.delta[p], small_table.G3, small_table.c_re,
+                              small_table.c_im, 3e-9, n)
+        for q, ball in enumerate((val, dd, dk)):
+            a, b = bounds(ball)
+            x = Fraction(float(hi[p, q])) + Fraction(float(lo[p, q]))
+            width = max(abs(float(b)), 1.0) * 1e-25
+            assert a - Fraction(width) <= x <= b + Fraction(width)
+            assert float(b - a) < 1e-30 * max(1.0, abs(float(a)))
+
+
 @pytest.mark.skipif(not RefLib.available(), reason="reference evaluator not built")
 def test_quad_oracle_matches_reference_evaluator(oracle, small_table):
     """K2 from the reference's compute_peak_AB + h0 (path1_eval_fast.cpp:15-53, :76-81) on the
