@@ -152,6 +152,27 @@ int mb_k2_fast(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_
                const double *delta, double k, double T, double tol, double *out_val, double *out_dd,
                double *out_dk, double *err_bound);
 
+/* ---- compatibility with the reference's libpath1_eval.so ---------------------------------
+ * Same names, signatures and host-array contracts as search/path1_eval_fast.cpp:15 and :58, so
+ * search/eval_tech1_600k.py, eval_tech2_hdrop_600k.py, eval_sub35_candidates.py and
+ * path1_kernel_opt.py can load this library instead.  Computed on the current CUDA device.
+ * The void forms (like the reference) cannot return a status: on failure they print the
+ * message to stderr and fill their outputs with NaN.  The mb_ forms return the status. */
+void compute_peak_AB(int n_peaks, const uint64_t *x_lo_arr, const uint64_t *x_hi_arr, const double *dy0_arr,
+                     int n_zeros, const double *alpha, const double *gamma, const uint64_t *ghi_lo,
+                     const uint64_t *ghi_hi, const uint64_t *glo_lo, const uint64_t *glo_hi,
+                     const uint64_t *psi_lo, const uint64_t *psi_hi, double *out_A, double *out_B);
+void polish_peaks_with_weights(int n_peaks, int n_zeros, const double *A, const double *B, const double *gamma,
+                               const double *w, double grid_half_width, int grid_steps, double *out_h_unpol,
+                               double *out_h_pol, double *out_ddy_pol);
+int mb_compute_peak_AB(int n_peaks, const uint64_t *x_lo_arr, const uint64_t *x_hi_arr, const double *dy0_arr,
+                       int n_zeros, const double *alpha, const double *gamma, const uint64_t *ghi_lo,
+                       const uint64_t *ghi_hi, const uint64_t *glo_lo, const uint64_t *glo_hi,
+                       const uint64_t *psi_lo, const uint64_t *psi_hi, double *out_A, double *out_B);
+int mb_polish_peaks_with_weights(int n_peaks, int n_zeros, const double *A, const double *B, const double *gamma,
+                                 const double *w, double grid_half_width, int grid_steps, double *out_h_unpol,
+                                 double *out_h_pol, double *out_ddy_pol);
+
 #ifdef __cplusplus
 }
 #endif
