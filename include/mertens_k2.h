@@ -147,6 +147,16 @@ int mb_plan_tier_terms(const mb_plan *p, double *heavy_terms, double *light_term
  * instructions per second: the peak against which the ALU-bound kernels are reported. */
 int mb_calibrate_issue(int device, double *thread_inst_per_s);
 
+/* Batched Newton polish of the offsets: h0 = K2 at the given d_delta; then up to `iters` steps
+ * delta -= clamp(K2'/K2'', +-max_step) with K2' = dK2/ddelta, K2'' = d2K2/ddelta2 = dK2/dk from
+ * the fused kernel; a candidate stops after |step| < 1e-13 or |K2''| <= 1e-12; the larger |K2|
+ * of start and end point is kept.  d_delta is updated in place; d_val/d_dd/d_dk hold the kept
+ * point's values.  Restates the Newton loop of search/path1_eval_fast.cpp:103-141 (there:
+ * 6 steps, clamp 1e-4) on the chosen form. */
+int mb_plan_newton_dev(mb_plan *p, const uint64_t *d_v_int, const uint64_t *d_v_frac, double *d_delta,
+                       int iters, double max_step, double *d_h0, double *d_val, double *d_dd, double *d_dk,
+                       void *stream);
+
 /* One-group convenience: plan, run, destroy.  *err_bound receives the a-priori bound. */
 int mb_k2_fast(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                const double *delta, double k, double T, double tol, double *out_val, double *out_dd,

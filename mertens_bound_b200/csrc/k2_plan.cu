@@ -34,6 +34,8 @@ struct mb_plan {
     double *d_delta = nullptr, *d_out = nullptr;
     void *h_pinned = nullptr;
     cudaGraphExec_t graph = nullptr;
+    DevBuf newton_buf;             // Newton polish: starting point, its gradients, stop flags
+    ~mb_plan() { newton_buf.release(); }
 };
 
 namespace {
@@ -376,6 +378,79 @@ extern "C" int mb_plan_run(mb_plan *p, const uint64_t *vi, const uint64_t *vf, c
     std::memcpy(val, o, P * 8);
     if (dd) std::memcpy(dd, o + P, P * 8);
     if (dk) std::memcpy(dk, o + 2 * P, P * 8);
+    return MB_OK;
+}
+
+// ------------------------------------------------------------------ batched Newton polish
+//
+// Per candidate (search/path1_eval_fast.cpp:103-141 restated on the fused kernel): h0 = K2 at the
+// starting delta; then up to `iters` steps delta -= clamp(K2'/K2'', +-max_step) where
+// K2' = dK2/ddelta and K2'' = d2K2/ddelta2 = dK2/dk (both returned by the fused kernel); a
+// candidate stops moving once |step| < 1e-13 or |K2''| <= 1e-12; finally the larger |h| of the
+// start and the end point is kept (with its delta).
+namespace {
+
+__global__ void newton_update_kernel(int64_t P, double *delta, const double *dd, const double *dk, double max_step,
+                                     unsigned char *done) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P || done[p]) return;
+    const double fpp = dk[p];
+    if (!(fabs(fpp) > 1e-12)) {
+        done[p] = 1;
+        return;
+    }
+    double step = fmin(fmax(dd[p] / fpp, -max_step), max_step);
+    delta[p] -= step;
+    if (fabs(step) < 1e-13) done[p] = 1;
+}
+
+__global__ void newton_choose_kernel(int64_t P, double *delta, const double *delta0, const double *h0, double *val,
+                                     double *dd, double *dk, const double *dd0, const double *dk0) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    if (fabs(h0[p]) > fabs(val[p])) {
+        val[p] = h0[p];
+        delta[p] = delta0[p];
+        dd[p] = dd0[p];
+        dk[p] = dk0[p];
+    }
+}
+
+}  // namespace
+
+extern "C" int mb_plan_newton_dev(mb_plan *p, const uint64_t *d_vi, const uint64_t *d_vf, double *d_delta,
+                                  int iters, double max_step, double *d_h0, double *d_val, double *d_dd,
+                                  double *d_dk, void *stream) {
+    MB_CHECK_ARG(p && d_vi && d_vf && d_delta && d_h0 && d_val && d_dd && d_dk, "mb_plan_newton_dev: null argument");
+    MB_CHECK_ARG(iters >= 0 && iters <= 1000, "mb_plan_newton_dev: iters=%d", iters);
+    MB_CHECK_ARG(std::isfinite(max_step) && max_step > 0, "mb_plan_newton_dev: max_step=%g", max_step);
+    MB_TRY(device_guard(p->table->device));
+    if (p->P == 0) return MB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t P = (size_t)p->P;
+    // plan-owned scratch: delta0, dd0, dk0 and the per-candidate stop flags
+    MB_TRY(p->newton_buf.ensure(3 * P * 8 + P + 256));
+    double *delta0 = (double *)p->newton_buf.p, *dd0 = delta0 + P, *dk0 = dd0 + P;
+    unsigned char *done = (unsigned char *)(dk0 + P);
+    const unsigned nb = (unsigned)((P + 255) / 256);
+    MB_CUDA(cudaMemcpyAsync(delta0, d_delta, P * 8, cudaMemcpyDeviceToDevice, s));
+    MB_CUDA(cudaMemsetAsync(done, 0, P, s));
+    MB_TRY(plan_run_dev(p, d_vi, d_vf, d_delta, d_h0, dd0, dk0, s));
+    const double *dd_in = dd0, *dk_in = dk0;
+    for (int it = 0; it < iters; ++it) {
+        newton_update_kernel<<<nb, 256, 0, s>>>(p->P, d_delta, dd_in, dk_in, max_step, done);
+        MB_CUDA(cudaGetLastError());
+        MB_TRY(plan_run_dev(p, d_vi, d_vf, d_delta, d_val, d_dd, d_dk, s));
+        dd_in = d_dd;
+        dk_in = d_dk;
+    }
+    if (iters == 0) {
+        MB_CUDA(cudaMemcpyAsync(d_val, d_h0, P * 8, cudaMemcpyDeviceToDevice, s));
+        MB_CUDA(cudaMemcpyAsync(d_dd, dd0, P * 8, cudaMemcpyDeviceToDevice, s));
+        MB_CUDA(cudaMemcpyAsync(d_dk, dk0, P * 8, cudaMemcpyDeviceToDevice, s));
+    }
+    newton_choose_kernel<<<nb, 256, 0, s>>>(p->P, d_delta, delta0, d_h0, d_val, d_dd, d_dk, dd0, dk0);
+    MB_CUDA(cudaGetLastError());
     return MB_OK;
 }
 
