@@ -162,6 +162,14 @@ int mb_k2_fast(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_
                const double *delta, double k, double T, double tol, double *out_val, double *out_dd,
                double *out_dk, double *err_bound);
 
+/* Grid scan: out_h[p * n_m + i] = K2(v_p + (m0 + i) step) for i < n_m, with step the 64.64
+ * fixed-point number step_int + step_frac 2^-64.  Every grid point's phase is exact
+ * (frac(y G) = frac(v G) + m frac(step G), 128-bit); sine/cosine and sums in FP64.
+ * Replaces the FP64 grid of search/polish.py:50-72 (phi + m dphi mod 2pi) and the grid stages
+ * of search/gpu_mertens_stream.cu:381-505 / path1_eval_fast.cpp:86-101. */
+int mb_grid_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k, double T,
+                 uint64_t step_int, uint64_t step_frac, int64_t m0, int64_t n_m, double *out_h);
+
 /* ---- compatibility with the reference's libpath1_eval.so ---------------------------------
  * Same names, signatures and host-array contracts as search/path1_eval_fast.cpp:15 and :58, so
  * search/eval_tech1_600k.py, eval_tech2_hdrop_600k.py, eval_sub35_candidates.py and

@@ -45,6 +45,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_calibrate_issue": (i32, [i32, f64p]),
     "mb_k2_plain_noalloc_dev": (i32, [vp, vp, vp, vp, i64, i64, i64, vp, vp, vp, f64, vp, vp, vp, vp]),
     "mb_k2_certified": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
+    "mb_grid_scan": (i32, [vp, i64, vp, vp, f64, f64, C.c_uint64, C.c_uint64, i64, i64, vp]),
     "compute_peak_AB": (None, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "polish_peaks_with_weights": (None, [i32, i32, vp, vp, vp, vp, f64, i32, vp, vp, vp]),
     "mb_compute_peak_AB": (i32, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),

@@ -152,6 +152,33 @@ MB_DEV void sincos_turns_half(double t, double &s2, double &c2) {
     c2 = fma(-2.0 * s, s, 1.0);
 }
 
+// 1.5 2^52: adding it rounds a double of magnitude < 2^51 to an integer held in the low
+// mantissa word.
+constexpr double MB_MAGIC = 6755399441055744.0;
+
+// sin/cos(2 pi y) for any y (turns) via quarter-turn reduction; FP64, error ~6e-14
+// (the degree-5 QUAD polynomials on |r| <= 1/8).
+MB_DEV void sincos_turns_quad(double y, double &sn, double &cs) {
+    double m = fma(y, 4.0, MB_MAGIC);
+    int q = __double2loint(m);
+    double r = fma(-0.25, m - MB_MAGIC, y);          // |r| <= 1/8 (exact)
+    double u = r * r;
+    double ps = QUAD_S[5];
+#pragma unroll
+    for (int k = 4; k >= 0; --k) ps = fma(ps, u, QUAD_S[k]);
+    double pc = QUAD_C[5];
+#pragma unroll
+    for (int k = 4; k >= 0; --k) pc = fma(pc, u, QUAD_C[k]);
+    double s = r * ps;
+    // rotate by q quarter turns: q=0 (s,c) 1 (c,-s) 2 (-s,-c) 3 (-c,s)
+    double S = (q & 1) ? pc : s;
+    double Cc = (q & 1) ? s : pc;
+    int sgn_s = (q & 2) << 30;
+    int sgn_c = ((q ^ (q >> 1)) & 1) << 31;
+    sn = __hiloint2double(__double2hiint(S) ^ sgn_s, __double2loint(S));
+    cs = __hiloint2double(__double2hiint(Cc) ^ sgn_c, __double2loint(Cc));
+}
+
 // ---------------------------------------------------------------- reductions
 
 MB_DEV double warp_sum_xor(double x, int width) {

@@ -130,28 +130,6 @@ MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandReg
         }
 }
 
-// sin/cos(2 pi y) for any y (turns) via quarter-turn reduction; FP64.
-MB_DEV void sincos_turns_quad(double y, double &sn, double &cs) {
-    double m = fma(y, 4.0, MAGIC);
-    int q = __double2loint(m);
-    double r = fma(-0.25, m - MAGIC, y);          // |r| <= 1/8 (exact)
-    double u = r * r;
-    double ps = QUAD_S[5];
-#pragma unroll
-    for (int k = 4; k >= 0; --k) ps = fma(ps, u, QUAD_S[k]);
-    double pc = QUAD_C[5];
-#pragma unroll
-    for (int k = 4; k >= 0; --k) pc = fma(pc, u, QUAD_C[k]);
-    double s = r * ps;
-    // rotate by q quarter turns: q=0 (s,c) 1 (c,-s) 2 (-s,-c) 3 (-c,s)
-    double S = (q & 1) ? pc : s;
-    double Cc = (q & 1) ? s : pc;
-    int sgn_s = (q & 2) << 30;
-    int sgn_c = ((q ^ (q >> 1)) & 1) << 31;
-    sn = __hiloint2double(__double2hiint(S) ^ sgn_s, __double2loint(S));
-    cs = __hiloint2double(__double2hiint(Cc) ^ sgn_c, __double2loint(Cc));
-}
-
 template <int CPT>
 MB_DEV void heavy_tile(const ZHeavy *tile, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
                        double (&acc)[CPT][3]) {
