@@ -42,19 +42,24 @@ UNIT = "zero-terms/s"
 T0, K_GAUSS, P_PER_GPU, TOL = 3e5, 3e-9, 4096, 1e-10
 WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 candidates v~3.5e18 "
             "per GPU, k=3e-9, K2 + dK2/ddelta + dK2/dk per candidate, a-priori |err| <= 1e-10")
-# Thread instructions per zero-term of the light-tier kernel (the dominant kernel), from the
-# ncu capture summarised in profiles/k2_light_kernel_search_scoring.md.
-LIGHT_INST_PER_TERM = 22.5
+# Thread instructions per zero-term of the light-tier kernel (the dominant kernel) for each
+# candidates-per-thread setting, from the ncu captures summarised in
+# profiles/k2_light_kernel_search_scoring.md.
+LIGHT_INST_PER_TERM = {2: 24.6, 3: 25.1, 4: 21.2}
+# DRAM bytes per light launch on this workload (same captures): reads of the zero tiles and
+# candidates; writes ~0.
+LIGHT_DRAM_BYTES = {2: 16517632, 3: 16416512, 4: 16380672}
 REF_SAMPLE_CANDS = 64
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the summary of the other workloads")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     return ap.parse_args()
 
@@ -72,7 +77,7 @@ class ClockSampler:
         self.f = open(self.path, "w")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={CLOCK_QUERY}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
@@ -211,6 +216,10 @@ def run_ours(args):
 
     plan = k2.Plan(table, [P], [K_GAUSS], [T0], tol=TOL)
     gi = plan.group_info(0)
+    from mertens_bound_b200.autotune import autotune
+    t_tune = time.perf_counter()
+    tuned = autotune(plan, reps=3, use_cache=False)
+    tune_s = time.perf_counter() - t_tune
 
     def fast(tiers=3):
         check(L.mb_plan_run_tiers_dev(plan.handle, tiers, vi.data_ptr(), vf.data_ptr(), dl.data_ptr(),
@@ -239,7 +248,8 @@ def run_ours(args):
     heavy_ms = statistics.median(timed(lambda: fast(1), 5, 1))
     ht, lt = C_double_pair(L.mb_plan_tier_terms, plan.handle)
     peak = C_double(L.mb_calibrate_issue, local)
-    light_achieved = LIGHT_INST_PER_TERM * lt / (light_ms * 1e-3)
+    inst_per_term = LIGHT_INST_PER_TERM[tuned["config"][0]]
+    light_achieved = inst_per_term * lt / (light_ms * 1e-3)
 
     # end to end through the host-pointer API (pinned H2D, graph, D2H), every step
     for _ in range(3):
@@ -261,14 +271,17 @@ def run_ours(args):
                    "tol": TOL, "heavy_zeros": gi["n_heavy"], "err_bound": gi["err_bound"],
                    "l2": "256 MB buffer written between timed steps (table 28 MB < L2)",
                    "parallelism": f"candidates sharded over {world} GPU(s), no collective on the data path",
-                   "wall_s_timed_region": wall_s},
+                   "wall_s_timed_region": wall_s,
+                   "autotuned": {"light_cpt": tuned["config"][0], "nzw_shift": tuned["config"][1],
+                                 "chunk_scale": tuned["config"][2], "tuning_s": tune_s}},
         "plain_fp64": {"value": world * plain_rate, "ms_per_step": statistics.median(plain_ms)},
         "speedup_vs_plain": world * plain_rate and value / (world * plain_rate),
         "max_abs_diff_vs_plain": {"val": float(diff[0]), "dd": float(diff[1]), "dk": float(diff[2])},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * P, "d2h_bytes_per_step": 3 * 8 * P},
         "roofline": {"bound": "issue", "kernel": "k2_light_kernel", "achieved": light_achieved / 1e12,
                      "peak": peak / 1e12, "unit": "T thread-inst/s", "frac": light_achieved / peak,
-                     "traffic": None, "per_term_inst": LIGHT_INST_PER_TERM, "light_ms": light_ms,
+                     "traffic": LIGHT_DRAM_BYTES[tuned["config"][0]], "traffic_unit": "bytes/launch",
+                     "per_term_inst": inst_per_term, "light_ms": light_ms,
                      "heavy_ms": heavy_ms, "light_terms": lt, "heavy_terms": ht,
                      "peak_source": "measured live: FFMA issue rate (mb_calibrate_issue); MEASURED_PEAKS.json "
                                     "has only HBM and bf16-tensor peaks, neither binds this kernel"},
@@ -283,10 +296,112 @@ def run_ours(args):
                                 "nproc": os.cpu_count()}
     plan.close()
     table.close()
+    if world == 1 and not args.no_workloads:
+        line["workloads"] = other_workloads(torch, dev, timed)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def other_workloads(torch, dev, timed):
+    """The other four workload shapes, measured briefly on the same GPU (summary numbers)."""
+    from mertens_bound_b200 import k2, synth, _lib
+    from mertens_bound_b200._lib import check
+    from mertens_bound_b200.autotune import autotune
+    L = _lib.lib()
+    sptr = torch.cuda.current_stream(dev).cuda_stream
+    out = {}
+
+    def dev_cands(c):
+        return (torch.from_numpy(c.v_int.view(np.int64).copy()).to(dev),
+                torch.from_numpy(c.v_frac.view(np.int64).copy()).to(dev),
+                torch.from_numpy(c.delta.copy()).to(dev))
+
+    def plain_run(t, vi, vf, dl, o, k, T, off=0, n=None):
+        n = vi.shape[0] if n is None else n
+        check(L.mb_k2_plain_dev(t.handle, n, vi[off:].data_ptr(), vf[off:].data_ptr(), dl[off:].data_ptr(), k, T,
+                                o[0, off:].data_ptr(), o[1, off:].data_ptr(), o[2, off:].data_ptr(), sptr))
+
+    def plan_run(plan, vi, vf, dl, o):
+        plan.run_dev(vi.data_ptr(), vf.data_ptr(), dl.data_ptr(), o[0].data_ptr(), o[1].data_ptr(),
+                     o[2].data_ptr(), sptr)
+
+    # small_plain: 64 candidates x 10,000 zeros, k = 3e-9
+    small = synth.make_table(10_000, seed=1)
+    c1 = synth.make_candidates(64, seed=2)
+    with k2.ZeroTable.from_data(small, device=dev.index) as t:
+        vi, vf, dl = dev_cands(c1)
+        o1 = torch.empty(3, 64, dtype=torch.float64, device=dev)
+        o2 = torch.empty_like(o1)
+        pm = statistics.median(timed(lambda: plain_run(t, vi, vf, dl, o1, 3e-9, math.inf), 20, 3))
+        with k2.Plan(t, [64], [3e-9], [math.inf], tol=TOL) as plan:
+            autotune(plan, reps=3, use_cache=False)
+            fm = statistics.median(timed(lambda: plan_run(plan, vi, vf, dl, o2), 20, 3))
+            eb = plan.group_info(0)["err_bound"]
+        terms = 64 * 10_000
+        out["small_plain"] = {"zero_terms": terms, "plain_ms": pm, "chosen_ms": fm,
+                              "plain_rate": terms / pm * 1e3, "chosen_rate": terms / fm * 1e3,
+                              "max_abs_diff": float((o2[0] - o1[0]).abs().max()), "err_bound": eb}
+
+    big = synth.make_table(2_325_572, seed=1)
+    with k2.ZeroTable.from_data(big, device=dev.index) as tb:
+        # certified_full: Peak2, all 2,325,572 zeros below 1.3e6, k = 1.5e-10
+        pk = synth.peak2_candidate()
+        k2.k2_certified(tb, pk, 1.5e-10, 1.3e6, v_rad=2.0 ** -64)
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            lo, hi, ab = k2.k2_certified(tb, pk, 1.5e-10, 1.3e6, v_rad=2.0 ** -64)
+            ts.append(time.perf_counter() - t0)
+        out["certified_full"] = {"zeros": tb.count_below(1.3e6), "seconds": statistics.median(ts),
+                                 "lo": float(lo[0]), "hi": float(hi[0]), "width": float(hi[0] - lo[0]),
+                                 "abs_sum_hi": float(ab[0])}
+
+        # batched_uneven: 16,384 candidates in 12 groups over T x k
+        counts, ks, Ts = synth.batched_uneven_groups()
+        c4 = synth.make_candidates(sum(counts), seed=4)
+        vi, vf, dl = dev_cands(c4)
+        o1 = torch.empty(3, c4.n, dtype=torch.float64, device=dev)
+        o2 = torch.empty_like(o1)
+        with k2.Plan(tb, counts, ks, Ts, tol=TOL) as plan:
+            tuned = autotune(plan, reps=2, use_cache=False)
+            fm = statistics.median(timed(lambda: plan_run(plan, vi, vf, dl, o2), 5, 2))
+            terms = plan.info()["zero_terms"]
+            bounds = [plan.group_info(g)["err_bound"] for g in range(len(counts))]
+
+            def plain_all():
+                off = 0
+                for c, k, T in zip(counts, ks, Ts):
+                    plain_run(tb, vi, vf, dl, o1, k, T, off, c)
+                    off += c
+            pm = statistics.median(timed(plain_all, 3, 1))
+        out["batched_uneven"] = {"zero_terms": terms, "groups": len(counts), "chosen_ms": fm, "plain_ms": pm,
+                                 "chosen_rate": terms / fm * 1e3, "plain_rate": terms / pm * 1e3,
+                                 "speedup_vs_plain": pm / fm, "max_abs_diff": float((o2[0] - o1[0]).abs().max()),
+                                 "max_err_bound": max(bounds), "autotuned": list(tuned["config"])}
+
+        # newton_polish: 1,024 candidates, T0 = 1.3e6, k = 1.5e-10, 8 Newton steps
+        c5 = synth.make_candidates(1024, seed=5)
+        vi, vf, dl = dev_cands(c5)
+        o2 = torch.empty(3, 1024, dtype=torch.float64, device=dev)
+        with k2.Plan(tb, [1024], [1.5e-10], [1.3e6], tol=TOL) as plan:
+            autotune(plan, reps=3, use_cache=False)
+            em = statistics.median(timed(lambda: plan_run(plan, vi, vf, dl, o2), 5, 2))
+            h4 = torch.empty(4, 1024, dtype=torch.float64, device=dev)
+            d = dl.clone()
+
+            def newton():
+                d.copy_(dl)
+                check(L.mb_plan_newton_dev(plan.handle, vi.data_ptr(), vf.data_ptr(), d.data_ptr(), 8, 1e-4,
+                                           h4[0].data_ptr(), h4[1].data_ptr(), h4[2].data_ptr(), h4[3].data_ptr(),
+                                           sptr))
+            nm = statistics.median(timed(newton, 3, 1))
+            terms = 1024.0 * tb.count_below(1.3e6)
+            gain = float((h4[1].abs() - h4[0].abs()).mean())
+        out["newton_polish"] = {"zero_terms_per_eval": terms, "eval_ms": em, "eval_rate": terms / em * 1e3,
+                                "newton8_ms": nm, "evals_per_newton": 10, "mean_abs_gain": gain}
+    return out
 
 
 def C_double(fn, *args):

@@ -127,6 +127,12 @@ int mb_plan_destroy(mb_plan *p);
 /* Override the tile shape of group g: cpt in {1,2,4} candidates per thread, nzw in {1,2,4,8}
  * warps splitting the zeros, chunk sizes in zeros (0 = automatic; multiples of 128 / 256). */
 int mb_plan_set_shape(mb_plan *p, int g, int cpt, int nzw, int64_t heavy_chunk, int64_t light_chunk);
+/* Plan-wide tile configuration, the autotuner's search space: light-kernel candidates per
+ * thread (2, 3, 4), extra doublings of each group's warp split (0..3), and a scale of the
+ * automatic work-item size (0.125..8).  Replaces per-group overrides. */
+int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, double chunk_scale);
+/* Median device time in ms of `reps` runs on synthetic candidates (for the autotuner). */
+int mb_plan_time(mb_plan *p, int reps, double *ms);
 int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, int *n_items);
 int mb_plan_group_info(const mb_plan *p, int g, int64_t *n_T, int64_t *n_heavy, double *err_bound,
                        double *sum_abs);

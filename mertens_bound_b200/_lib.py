@@ -35,6 +35,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_plan_destroy": (i32, [vp]),
     "mb_plan_set_shape": (i32, [vp, i32, i32, i32, i64, i64]),
     "mb_plan_info": (i32, [vp, i64p, f64p, C.POINTER(i32)]),
+    "mb_plan_configure": (i32, [vp, i32, i32, f64]),
+    "mb_plan_time": (i32, [vp, i32, f64p]),
     "mb_plan_group_info": (i32, [vp, i32, i64p, i64p, f64p, f64p]),
     "mb_plan_run_dev": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "mb_plan_run": (i32, [vp, vp, vp, vp, vp, vp, vp]),

@@ -304,22 +304,35 @@ k2_light_kernel(TabView t, CandView c, const FastItem *items, const FastGroup *g
     light_item<CPT>(it, groups[it.group], t, c, partial, smem);
 }
 
-// Per candidate: sum the partials of its group's chunks in chunk order (deterministic).
+// One warp per candidate: lane l sums chunks l, l+32, ... of the candidate's group, then a fixed
+// shuffle tree adds the lanes (deterministic: the order depends only on the chunk count).
 __global__ void fast_reduce_kernel(const FastGroup *groups, int n_groups, const double *partial,
                                    int64_t P, double *val, double *dd, double *dk) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (p >= P) return;
-    int g = 0;
-    while (g + 1 < n_groups && groups[g + 1].c0 <= p) ++g;
-    const FastGroup gr = groups[g];
+    int lo = 0, hi = n_groups - 1;                 // group containing p (groups sorted by c0)
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (groups[mid].c0 <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    const FastGroup gr = groups[lo];
     double s0 = 0, s1 = 0, s2 = 0;
-    for (int ch = 0; ch < gr.n_chunks; ++ch) {
+    for (int ch = lane; ch < gr.n_chunks; ch += 32) {
         const double *o = partial + gr.pbase + ((int64_t)ch * gr.nc + (p - gr.c0)) * 3;
         s0 += o[0]; s1 += o[1]; s2 += o[2];
     }
-    val[p] = s0;
-    dd[p] = s1;
-    dk[p] = s2;
+    for (int off = 16; off > 0; off >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+    }
+    if (lane == 0) {
+        val[p] = s0;
+        dd[p] = s1;
+        dk[p] = s2;
+    }
 }
 
 static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cudaStream_t s) {
@@ -354,7 +367,7 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
     }
     if (light) MB_TRY(launch_light(tv, pd, c, s));
     if (heavy) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
-    fast_reduce_kernel<<<(unsigned)((c.P + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
+    fast_reduce_kernel<<<(unsigned)((c.P * 32 + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
                                                                      d_val, d_dd, d_dk);
     MB_CUDA(cudaGetLastError());
     return MB_OK;

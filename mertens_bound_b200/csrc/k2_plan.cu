@@ -25,6 +25,8 @@ struct mb_plan {
     std::vector<int> shape_nzw;
     std::vector<int64_t> heavy_chunk, light_chunk;
     int light_cpt = 4;
+    int nzw_shift = 0;             // extra doublings of the default warps-per-candidate-set split
+    double chunk_scale = 1.0;      // multiplies the automatic work-item sizes
     int n_heavy_items = 0;
     double zero_terms = 0;
     FastPlanDev dev;
@@ -108,8 +110,8 @@ int build_items(mb_plan *p, int sms) {
         Wl += (double)p->counts[g] * (p->n_T[g] - p->n_heavy[g]);
     }
     // ~4 items per heavy CTA (one per SM) and ~6 waves of light CTAs (about 3 per SM)
-    const double target_h = std::max(Wh / (4.0 * sms), 1.0);
-    const double target_l = std::max(Wl / (18.0 * sms), 1.0);
+    const double target_h = std::max(p->chunk_scale * Wh / (4.0 * sms), 1.0);
+    const double target_l = std::max(p->chunk_scale * Wl / (18.0 * sms), 1.0);
     std::vector<FastItem> heavy, light;
     int64_t c0 = 0, pbase = 0;
     for (int g = 0; g < p->n_groups; ++g) {
@@ -301,6 +303,71 @@ extern "C" int mb_plan_set_shape(mb_plan *p, int g, int cpt, int nzw, int64_t he
     p->light_chunk[g] = light_chunk;
     MB_TRY(device_guard(p->table->device));
     return upload(p);
+}
+
+// Plan-wide tile configuration (the autotuner's search space): light_cpt candidates per thread
+// in the light kernel (2, 3, 4), nzw_shift extra doublings of every group's warp split (0..3,
+// capped at 8 warps), chunk_scale times the automatic work-item size (0.125 .. 8).  Per-group
+// overrides set with mb_plan_set_shape are replaced.
+extern "C" int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, double chunk_scale) {
+    MB_CHECK_ARG(p, "mb_plan_configure: null plan");
+    MB_CHECK_ARG(light_cpt == 2 || light_cpt == 3 || light_cpt == 4, "mb_plan_configure: light_cpt=%d", light_cpt);
+    MB_CHECK_ARG(nzw_shift >= 0 && nzw_shift <= 3, "mb_plan_configure: nzw_shift=%d", nzw_shift);
+    MB_CHECK_ARG(chunk_scale >= 0.125 && chunk_scale <= 8.0, "mb_plan_configure: chunk_scale=%g", chunk_scale);
+    p->light_cpt = light_cpt;
+    p->nzw_shift = nzw_shift;
+    p->chunk_scale = chunk_scale;
+    for (int g = 0; g < p->n_groups; ++g) {
+        p->shape_nzw[g] = std::min(8, default_nzw(p->counts[g], light_cpt) << nzw_shift);
+        p->heavy_chunk[g] = 0;
+        p->light_chunk[g] = 0;
+    }
+    MB_TRY(device_guard(p->table->device));
+    return upload(p);
+}
+
+// Median device time (ms) of `reps` runs of the plan on synthetic candidates (the values do not
+// change the work), after one warm-up run.  Used by the autotuner.
+extern "C" int mb_plan_time(mb_plan *p, int reps, double *ms) {
+    MB_CHECK_ARG(p && ms && reps >= 1 && reps <= 1000, "mb_plan_time: bad argument");
+    MB_TRY(device_guard(p->table->device));
+    if (p->P == 0) {
+        *ms = 0.0;
+        return MB_OK;
+    }
+    MB_TRY(ensure_io(p));
+    const size_t P = (size_t)p->P;
+    std::vector<uint64_t> v(2 * P);
+    uint64_t x = 0x9E3779B97F4A7C15ull;
+    for (size_t i = 0; i < 2 * P; ++i) {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        v[i] = (i < P) ? 3400000000000000000ull + (x % 200000000000000000ull) : x;
+    }
+    cudaStream_t s = p->table->stream;
+    MB_CUDA(cudaMemcpyAsync(p->d_vi, v.data(), P * 8, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(p->d_vf, v.data() + P, P * 8, cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaMemsetAsync(p->d_delta, 0, P * 8, s));
+    cudaEvent_t e0, e1;
+    MB_CUDA(cudaEventCreate(&e0));
+    MB_CUDA(cudaEventCreate(&e1));
+    std::vector<float> t;
+    int st = plan_run_dev(p, p->d_vi, p->d_vf, p->d_delta, p->d_out, p->d_out + P, p->d_out + 2 * P, s);
+    for (int r = 0; r < reps && st == MB_OK; ++r) {
+        cudaEventRecord(e0, s);
+        st = plan_run_dev(p, p->d_vi, p->d_vf, p->d_delta, p->d_out, p->d_out + P, p->d_out + 2 * P, s);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float m = 0;
+        cudaEventElapsedTime(&m, e0, e1);
+        t.push_back(m);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MB_TRY(st);
+    MB_CUDA(cudaGetLastError());
+    std::sort(t.begin(), t.end());
+    *ms = t[t.size() / 2];
+    return MB_OK;
 }
 
 extern "C" int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, int *n_items) {

@@ -137,6 +137,21 @@ class Plan:
     def set_shape(self, g: int, cpt: int, nzw: int, heavy_chunk: int = 0, light_chunk: int = 0):
         check(_lib.lib().mb_plan_set_shape(self.handle, g, cpt, nzw, heavy_chunk, light_chunk))
 
+    def configure(self, light_cpt: int, nzw_shift: int, chunk_scale: float):
+        check(_lib.lib().mb_plan_configure(self.handle, int(light_cpt), int(nzw_shift), float(chunk_scale)))
+        self.config = (int(light_cpt), int(nzw_shift), float(chunk_scale))
+
+    def time(self, reps: int = 3) -> float:
+        """Median device milliseconds of one run (synthetic candidates)."""
+        ms = C.c_double()
+        check(_lib.lib().mb_plan_time(self.handle, int(reps), C.byref(ms)))
+        return ms.value
+
+    def tier_terms(self):
+        h, l = C.c_double(), C.c_double()
+        check(_lib.lib().mb_plan_tier_terms(self.handle, C.byref(h), C.byref(l)))
+        return h.value, l.value
+
     def info(self):
         P, zt, ni = C.c_int64(), C.c_double(), C.c_int()
         check(_lib.lib().mb_plan_info(self.handle, C.byref(P), C.byref(zt), C.byref(ni)))

@@ -174,6 +174,16 @@ def peak2_candidate() -> Candidates:
                       np.zeros(1, dtype=np.float64))
 
 
+def batched_uneven_groups():
+    """The batched workload: 12 groups of unequal size (64..4096, 16,384 candidates in all), one
+    per (T, k) in {1e5, 3e5, 6e5, 1.3e6} x {3e-9, 1e-9, 1.5e-10}.  Returns (counts, ks, Ts)."""
+    counts = [4096, 64, 2048, 256, 3072, 128, 1536, 512, 1024, 2048, 1024, 576]
+    Ts = [T for T in (1e5, 3e5, 6e5, 1.3e6) for _ in range(3)]
+    ks = [k for _ in range(4) for k in (3e-9, 1e-9, 1.5e-10)]
+    assert sum(counts) == 16_384 and min(counts) >= 64 and max(counts) <= 4096
+    return counts, ks, Ts
+
+
 # The five workloads (sizes, cutoffs and Gaussian widths) the evaluator is measured on.
 WORKLOADS = {
     "small_plain": dict(n_zeros=10_000, T=math.inf, k=3e-9, P=64, table_seed=1, cand_seed=2),
