@@ -92,6 +92,14 @@ int mb_k2_certified(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_
                     const double *v_rad, double k, double T, const double *term_rad, double *out_lo,
                     double *out_hi, double *out_abs_hi);
 
+/* Certified interval over the zeros [j0, j1) only, for k anywhere in [k_lo, k_hi] (a decimal
+ * k such as 1.5e-10 is enclosed by its two neighbouring doubles).  term_rad (nullable) has
+ * j1 - j0 entries.  The batch sum of certify_K2.work (certification/certify_K2.py:100-133) for
+ * zeros n0 .. n0 + num - 1 is j0 = n0 - 1, j1 = n0 - 1 + num. */
+int mb_k2_certified_range(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                          const double *v_rad, double k_lo, double k_hi, int64_t j0, int64_t j1,
+                          const double *term_rad, double *out_lo, double *out_hi, double *out_abs_hi);
+
 /* Plain FP64 K2 for callers that cannot allocate device memory: no counterpart in the
  * reference (its evaluator is host code).  Callers in a host callback, inside a fixed memory
  * budget or in a runtime that owns every allocation cannot call cudaMalloc; this entry point
@@ -131,6 +139,11 @@ int mb_plan_set_shape(mb_plan *p, int g, int cpt, int nzw, int64_t heavy_chunk, 
  * thread (2, 3, 4), extra doublings of each group's warp split (0..3), and a scale of the
  * automatic work-item size (0.125..8).  Replaces per-group overrides. */
 int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, double chunk_scale);
+/* Restrict every group to the zeros [j0, j1) of its [0, count_below(T)): one shard of a
+ * zero-range split across GPUs; the shards' results add up to the whole sum (tier boundaries and
+ * error bounds are those of the whole sum).  No reference counterpart (the reference shards zero
+ * batches over a process pool, certification/certify_K2.py:160-174). */
+int mb_plan_set_zero_range(mb_plan *p, int64_t j0, int64_t j1);
 /* Median device time in ms of `reps` runs on synthetic candidates (for the autotuner). */
 int mb_plan_time(mb_plan *p, int reps, double *ms);
 int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, int *n_items);

@@ -36,6 +36,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_plan_set_shape": (i32, [vp, i32, i32, i32, i64, i64]),
     "mb_plan_info": (i32, [vp, i64p, f64p, C.POINTER(i32)]),
     "mb_plan_configure": (i32, [vp, i32, i32, f64]),
+    "mb_plan_set_zero_range": (i32, [vp, i64, i64]),
     "mb_plan_time": (i32, [vp, i32, f64p]),
     "mb_plan_group_info": (i32, [vp, i32, i64p, i64p, f64p, f64p]),
     "mb_plan_run_dev": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
@@ -47,6 +48,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_calibrate_issue": (i32, [i32, f64p]),
     "mb_k2_plain_noalloc_dev": (i32, [vp, vp, vp, vp, i64, i64, i64, vp, vp, vp, f64, vp, vp, vp, vp]),
     "mb_k2_certified": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
+    "mb_k2_certified_range": (i32, [vp, i64, vp, vp, vp, f64, f64, i64, i64, vp, vp, vp, vp]),
     "mb_grid_scan": (i32, [vp, i64, vp, vp, f64, f64, C.c_uint64, C.c_uint64, i64, i64, vp]),
     "compute_peak_AB": (None, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "polish_peaks_with_weights": (None, [i32, i32, vp, vp, vp, vp, f64, i32, vp, vp, vp]),

@@ -91,8 +91,9 @@ struct CertTerm {
     double abs_hi;
 };
 
-MB_DEV CertTerm cert_term(const TabView &tv, int64_t j, uint64_t vi, uint64_t vf, double k, double v_rad,
-                          const double *term_rad) {
+// Term j; k lies in [k_lo, k_hi]; term_rad (nullable) is the per-term radius at index jr.
+MB_DEV CertTerm cert_term(const TabView &tv, int64_t j, uint64_t vi, uint64_t vf, double k_lo, double k_hi,
+                          double v_rad, const double *term_rad, int64_t jr) {
     uint64_t hi, lo;
     phase128_exact((uint32_t)vf, (uint32_t)(vf >> 32), (uint32_t)vi, (uint32_t)(vi >> 32), tv.g0[j], tv.g1[j],
                    tv.g2[j], tv.g3[j], tv.g4[j], hi, lo);
@@ -126,7 +127,7 @@ MB_DEV CertTerm cert_term(const TabView &tv, int64_t j, uint64_t vi, uint64_t vf
     const Ival A{__dsub_rd(a1.lo, a2.hi), __dsub_ru(a1.hi, a2.lo)};
     const double g = tv.gamma[j];
     const double glo = __dmul_rd(g, 1.0 - 8.881784197001252e-16), ghi = __dmul_ru(g, 1.0 + 8.881784197001252e-16);
-    const double ylo = __dmul_rd(__dmul_rd(k, glo), glo), yhi = __dmul_ru(__dmul_ru(k, ghi), ghi);
+    const double ylo = __dmul_rd(__dmul_rd(k_lo, glo), glo), yhi = __dmul_ru(__dmul_ru(k_hi, ghi), ghi);
     const Ival w = iv_exp_neg(ylo, yhi);
     Ival t = iv_wmul(w, A);
     t.lo *= 2.0;
@@ -134,7 +135,7 @@ MB_DEV CertTerm cert_term(const TabView &tv, int64_t j, uint64_t vi, uint64_t vf
     const double cabs = __dsqrt_ru(__fma_ru(cr, cr, __dmul_ru(ci, ci)));
     double rad = 0.0;
     if (v_rad > 0.0) rad = __dmul_ru(__dmul_ru(cabs, ghi), v_rad);
-    if (term_rad) rad = __dadd_ru(rad, term_rad[j]);
+    if (term_rad) rad = __dadd_ru(rad, term_rad[jr]);
     if (rad > 0.0) {
         const double wr = __dmul_ru(2.0 * w.hi, rad);
         t.lo = __dsub_rd(t.lo, wr);
@@ -147,14 +148,14 @@ constexpr int CERT_THREADS = 256;
 
 // grid (zero blocks, candidates); partial[(blockIdx.x * P + p) * 3 + {lo, hi, abs_hi}]
 __global__ void __launch_bounds__(CERT_THREADS)
-k2_certified_kernel(TabView tv, const uint64_t *vi, const uint64_t *vf, const double *v_rad, int64_t P, int64_t n_use,
-                    double k, const double *term_rad, double *partial) {
+k2_certified_kernel(TabView tv, const uint64_t *vi, const uint64_t *vf, const double *v_rad, int64_t P, int64_t j0,
+                    int64_t j1, double k_lo, double k_hi, const double *term_rad, double *partial) {
     const int64_t p = blockIdx.y;
     const uint64_t a = vi[p], b = vf[p];
     const double vr = v_rad ? v_rad[p] : 0.0;
     double slo = 0.0, shi = 0.0, sab = 0.0;
-    for (int64_t j = (int64_t)blockIdx.x * CERT_THREADS + threadIdx.x; j < n_use; j += (int64_t)gridDim.x * CERT_THREADS) {
-        CertTerm ct = cert_term(tv, j, a, b, k, vr, term_rad);
+    for (int64_t jr = (int64_t)blockIdx.x * CERT_THREADS + threadIdx.x; j0 + jr < j1; jr += (int64_t)gridDim.x * CERT_THREADS) {
+        CertTerm ct = cert_term(tv, j0 + jr, a, b, k_lo, k_hi, vr, term_rad, jr);
         slo = __dadd_rd(slo, ct.t.lo);
         shi = __dadd_ru(shi, ct.t.hi);
         sab = __dadd_ru(sab, ct.abs_hi);
@@ -203,9 +204,10 @@ __global__ void certified_reduce_kernel(const double *partial, int64_t P, int nb
 }
 
 int launch_certified(Table &t, const uint64_t *d_vi, const uint64_t *d_vf, const double *d_vrad, int64_t P,
-                     int64_t n_use, double k, const double *d_term_rad, double *d_lo, double *d_hi,
-                     double *d_abs, cudaStream_t s) {
+                     int64_t j0, int64_t j1, double k_lo, double k_hi, const double *d_term_rad, double *d_lo,
+                     double *d_hi, double *d_abs, cudaStream_t s) {
     if (P == 0) return MB_OK;
+    const int64_t n_use = std::max<int64_t>(0, j1 - j0);
     int sms = 148;
     MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t.device));
     int64_t want = std::max<int64_t>(1, ((int64_t)sms * 8 + P - 1) / P);
@@ -214,7 +216,8 @@ int launch_certified(Table &t, const uint64_t *d_vi, const uint64_t *d_vf, const
     MB_TRY(t.work.ensure((size_t)nblk * P * 3 * sizeof(double)));
     double *partial = (double *)t.work.p;
     dim3 grid((unsigned)nblk, (unsigned)P);
-    k2_certified_kernel<<<grid, CERT_THREADS, 0, s>>>(view(t), d_vi, d_vf, d_vrad, P, n_use, k, d_term_rad, partial);
+    k2_certified_kernel<<<grid, CERT_THREADS, 0, s>>>(view(t), d_vi, d_vf, d_vrad, P, j0, j1, k_lo, k_hi, d_term_rad,
+                                                      partial);
     MB_CUDA(cudaGetLastError());
     certified_reduce_kernel<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(partial, P, (int)nblk, d_lo, d_hi, d_abs);
     MB_CUDA(cudaGetLastError());
@@ -225,22 +228,25 @@ int launch_certified(Table &t, const uint64_t *d_vi, const uint64_t *d_vf, const
 
 using namespace mb;
 
-extern "C" int mb_k2_certified(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
-                               const double *v_rad, double k, double T, const double *term_rad,
-                               double *out_lo, double *out_hi, double *out_abs_hi) {
-    MB_CHECK_ARG(h && v_int && v_frac && out_lo && out_hi, "mb_k2_certified: null argument");
-    MB_CHECK_ARG(P >= 0 && P <= 65535, "mb_k2_certified: P=%lld out of range (0..65535)", (long long)P);
-    MB_CHECK_ARG(std::isfinite(k) && k >= 0.0, "mb_k2_certified: k=%g", k);
-    MB_CHECK_ARG(!std::isnan(T), "mb_k2_certified: T is NaN");
+extern "C" int mb_k2_certified_range(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                                     const double *v_rad, double k_lo, double k_hi, int64_t j0, int64_t j1,
+                                     const double *term_rad, double *out_lo, double *out_hi, double *out_abs_hi) {
+    MB_CHECK_ARG(h && v_int && v_frac && out_lo && out_hi, "mb_k2_certified_range: null argument");
+    MB_CHECK_ARG(P >= 0 && P <= 65535, "mb_k2_certified_range: P=%lld out of range (0..65535)", (long long)P);
+    MB_CHECK_ARG(std::isfinite(k_lo) && std::isfinite(k_hi) && 0.0 <= k_lo && k_lo <= k_hi,
+                 "mb_k2_certified_range: k interval [%g, %g]", k_lo, k_hi);
     if (P == 0) return MB_OK;
     Table &t = table_of(h);
-    const int64_t n_use = t.count_below(T);
+    MB_CHECK_ARG(0 <= j0 && j0 <= j1 && j1 <= t.n, "mb_k2_certified_range: zero range [%lld, %lld) of %lld",
+                 (long long)j0, (long long)j1, (long long)t.n);
+    const int64_t n_use = j1 - j0;
     if (v_rad)
         for (int64_t p = 0; p < P; ++p)
-            MB_CHECK_ARG(std::isfinite(v_rad[p]) && v_rad[p] >= 0.0, "mb_k2_certified: v_rad[%lld]", (long long)p);
+            MB_CHECK_ARG(std::isfinite(v_rad[p]) && v_rad[p] >= 0.0, "mb_k2_certified_range: v_rad[%lld]", (long long)p);
     if (term_rad)
         for (int64_t j = 0; j < n_use; ++j)
-            MB_CHECK_ARG(std::isfinite(term_rad[j]) && term_rad[j] >= 0.0, "mb_k2_certified: term_rad[%lld]", (long long)j);
+            MB_CHECK_ARG(std::isfinite(term_rad[j]) && term_rad[j] >= 0.0, "mb_k2_certified_range: term_rad[%lld]",
+                         (long long)j);
     MB_TRY(device_guard(t.device));
     const size_t cb = (size_t)P * 8, rb = term_rad ? (size_t)n_use * 8 : 0;
     MB_TRY(t.io.ensure(6 * cb + rb + 256));
@@ -252,11 +258,21 @@ extern "C" int mb_k2_certified(mb_table *h, int64_t P, const uint64_t *v_int, co
     MB_CUDA(cudaMemcpyAsync(d_vf, v_frac, cb, cudaMemcpyHostToDevice, t.stream));
     if (v_rad) MB_CUDA(cudaMemcpyAsync(d_vrad, v_rad, cb, cudaMemcpyHostToDevice, t.stream));
     if (term_rad && rb) MB_CUDA(cudaMemcpyAsync(d_rad, term_rad, rb, cudaMemcpyHostToDevice, t.stream));
-    MB_TRY(launch_certified(t, d_vi, d_vf, v_rad ? d_vrad : nullptr, P, n_use, k, d_rad, d_out, d_out + P,
+    MB_TRY(launch_certified(t, d_vi, d_vf, v_rad ? d_vrad : nullptr, P, j0, j1, k_lo, k_hi, d_rad, d_out, d_out + P,
                             d_out + 2 * P, t.stream));
     MB_CUDA(cudaMemcpyAsync(out_lo, d_out, cb, cudaMemcpyDeviceToHost, t.stream));
     MB_CUDA(cudaMemcpyAsync(out_hi, d_out + P, cb, cudaMemcpyDeviceToHost, t.stream));
     if (out_abs_hi) MB_CUDA(cudaMemcpyAsync(out_abs_hi, d_out + 2 * P, cb, cudaMemcpyDeviceToHost, t.stream));
     MB_CUDA(cudaStreamSynchronize(t.stream));
     return MB_OK;
+}
+
+extern "C" int mb_k2_certified(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                               const double *v_rad, double k, double T, const double *term_rad,
+                               double *out_lo, double *out_hi, double *out_abs_hi) {
+    MB_CHECK_ARG(h, "mb_k2_certified: null table");
+    MB_CHECK_ARG(std::isfinite(k) && k >= 0.0, "mb_k2_certified: k=%g", k);
+    MB_CHECK_ARG(!std::isnan(T), "mb_k2_certified: T is NaN");
+    return mb_k2_certified_range(h, P, v_int, v_frac, v_rad, k, k, 0, table_of(h).count_below(T), term_rad, out_lo,
+                                 out_hi, out_abs_hi);
 }

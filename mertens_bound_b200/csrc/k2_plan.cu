@@ -27,6 +27,7 @@ struct mb_plan {
     int light_cpt = 4;
     int nzw_shift = 0;             // extra doublings of the default warps-per-candidate-set split
     double chunk_scale = 1.0;      // multiplies the automatic work-item sizes
+    int64_t z_begin = 0, z_end = INT64_MAX;   // zero-range shard of every group (default: all)
     int n_heavy_items = 0;
     double zero_terms = 0;
     FastPlanDev dev;
@@ -104,10 +105,15 @@ int build_items(mb_plan *p, int sms) {
     p->groups.clear();
     p->items.clear();
     p->zero_terms = 0;
+    // the zeros this plan evaluates: [zb, ze) within each group's [0, n_T) (a zero-range shard)
+    auto hb = [&](int g) { return std::max<int64_t>(0, p->z_begin); };
+    auto he = [&](int g) { return std::min(p->n_heavy[g], p->z_end); };
+    auto lb = [&](int g) { return std::max(p->n_heavy[g], p->z_begin); };
+    auto le = [&](int g) { return std::min(p->n_T[g], p->z_end); };
     double Wh = 0, Wl = 0;
     for (int g = 0; g < p->n_groups; ++g) {
-        Wh += (double)p->counts[g] * p->n_heavy[g];
-        Wl += (double)p->counts[g] * (p->n_T[g] - p->n_heavy[g]);
+        Wh += (double)p->counts[g] * std::max<int64_t>(0, he(g) - hb(g));
+        Wl += (double)p->counts[g] * std::max<int64_t>(0, le(g) - lb(g));
     }
     // ~4 items per heavy CTA (one per SM) and ~6 waves of light CTAs (about 3 per SM)
     const double target_h = std::max(p->chunk_scale * Wh / (4.0 * sms), 1.0);
@@ -146,12 +152,12 @@ int build_items(mb_plan *p, int sms) {
             }
             ++ch;
         };
-        for (int64_t z = 0; z < p->n_heavy[g]; z += hz)
-            emit(z, std::min(z + hz, p->n_heavy[g]), 0, CTh, HEAVY_CPT, heavy);
-        for (int64_t z = p->n_heavy[g]; z < p->n_T[g]; z += lz)
-            emit(z, std::min(z + lz, p->n_T[g]), 1, CTl, p->light_cpt, light);
+        for (int64_t z = hb(g); z < he(g); z += hz)
+            emit(z, std::min(z + hz, he(g)), 0, CTh, HEAVY_CPT, heavy);
+        for (int64_t z = lb(g); z < le(g); z += lz)
+            emit(z, std::min(z + lz, le(g)), 1, CTl, p->light_cpt, light);
         gr.n_chunks = ch;
-        p->zero_terms += (double)gr.nc * p->n_T[g];
+        p->zero_terms += (double)gr.nc * (std::max<int64_t>(0, he(g) - hb(g)) + std::max<int64_t>(0, le(g) - lb(g)));
         pbase += (int64_t)gr.n_chunks * gr.nc * 3;
         c0 += gr.nc;
         p->groups.push_back(gr);
@@ -322,6 +328,17 @@ extern "C" int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, doubl
         p->heavy_chunk[g] = 0;
         p->light_chunk[g] = 0;
     }
+    MB_TRY(device_guard(p->table->device));
+    return upload(p);
+}
+
+// Restrict every group to the zeros [j0, j1) (intersected with its [0, n_T)): a zero-range shard.
+// Tier boundaries and error bounds stay those of the whole sum; the shards' results add up to it.
+extern "C" int mb_plan_set_zero_range(mb_plan *p, int64_t j0, int64_t j1) {
+    MB_CHECK_ARG(p, "mb_plan_set_zero_range: null plan");
+    MB_CHECK_ARG(0 <= j0 && j0 <= j1, "mb_plan_set_zero_range: [%lld, %lld)", (long long)j0, (long long)j1);
+    p->z_begin = j0;
+    p->z_end = j1;
     MB_TRY(device_guard(p->table->device));
     return upload(p);
 }

@@ -74,6 +74,24 @@ def test_plan_shapes_agree(table):
             assert np.max(np.abs(v - ref)) <= 2 * eb
 
 
+def test_zero_range_shards_add_up(table):
+    """Zero-range shards (one per GPU in a zero-sharded run) sum to the whole evaluation."""
+    from mertens_bound_b200 import distributed
+    from mertens_bound_b200._lib import check, lib
+    cd = synth.make_candidates(200, seed=12)
+    with k2.Plan(table, [200], [3e-9], [math.inf], tol=TOL) as plan:
+        full = np.stack(plan.run(cd), axis=1)
+        eb = plan.group_info(0)["err_bound"]
+        parts = []
+        for r in range(3):
+            j0, j1 = distributed.shard_range(table.n, 3, r)
+            check(lib().mb_plan_set_zero_range(plan.handle, j0, j1))
+            parts.append(np.stack(plan.run(cd), axis=1))
+    tot = sum(parts)
+    assert np.max(np.abs(tot[:, 0] - full[:, 0])) <= 2 * eb
+    assert np.max(np.abs(tot[:, 1] - full[:, 1])) <= 1e-9 * np.max(np.abs(full[:, 1]))
+
+
 def test_all_heavy_when_tolerance_tight(table, small_table, oracle):
     cd = synth.make_candidates(16, seed=10)
     with k2.Plan(table, [16], [3e-9], [math.inf], tol=1e-14) as plan:
