@@ -189,6 +189,13 @@ int mb_k2_fast(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_
 int mb_grid_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k, double T,
                  uint64_t step_int, uint64_t step_frac, int64_t m0, int64_t n_m, double *out_h);
 
+/* Many small grids: out_h[p * n_m + i] = K2 over the first n_use zeros at v_p + (m0 + i) step,
+ * n_m <= 1024, one CTA per base point.  The stage scans of the enumerators' hit polish
+ * (search/gpu_mertens_stream.cu:381-505 ZeroData::polish, search/fast_mertens_enum.cpp:145-276:
+ * 256, 512, 2048, 15000 and all zeros at decreasing steps) are calls of this. */
+int mb_hit_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k, int64_t n_use,
+                uint64_t step_int, uint64_t step_frac, int64_t m0, int64_t n_m, double *out_h);
+
 /* ---- compatibility with the reference's libpath1_eval.so ---------------------------------
  * Same names, signatures and host-array contracts as search/path1_eval_fast.cpp:15 and :58, so
  * search/eval_tech1_600k.py, eval_tech2_hdrop_600k.py, eval_sub35_candidates.py and

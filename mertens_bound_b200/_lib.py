@@ -50,6 +50,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_k2_certified": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
     "mb_k2_certified_range": (i32, [vp, i64, vp, vp, vp, f64, f64, i64, i64, vp, vp, vp, vp]),
     "mb_grid_scan": (i32, [vp, i64, vp, vp, f64, f64, C.c_uint64, C.c_uint64, i64, i64, vp]),
+    "mb_hit_scan": (i32, [vp, i64, vp, vp, f64, i64, C.c_uint64, C.c_uint64, i64, i64, vp]),
     "compute_peak_AB": (None, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "polish_peaks_with_weights": (None, [i32, i32, vp, vp, vp, vp, f64, i32, vp, vp, vp]),
     "mb_compute_peak_AB": (i32, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),

@@ -92,6 +92,69 @@ k2_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, u
     }
 }
 
+// Small grids over many base points (the hit polish of the enumerators): one CTA per base point,
+// threads over zeros; for each zero the exact phase at the base point and the exact increment
+// per grid step, then every grid point in turn: warp-shuffle sum of the 32 lanes' terms, added
+// by lane 0 to its warp's row of shared accumulators (fixed order -> deterministic).
+constexpr int HIT_THREADS = 256;
+constexpr int HIT_MAX_M = 1024;
+
+__global__ void __launch_bounds__(HIT_THREADS)
+k2_hit_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, uint64_t sf, int64_t m0, int n_m,
+                   int64_t n_use, double k, double *out_h) {
+    extern __shared__ double acc[];            // [HIT_THREADS / 32][n_m]
+    const int p = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < (HIT_THREADS / 32) * n_m; i += HIT_THREADS) acc[i] = 0.0;
+    __syncthreads();
+    const uint64_t a_int = vi[p], a_frac = vf[p];
+    const uint32_t mabs = (uint32_t)(m0 < 0 ? -m0 : m0);
+    const int64_t rounds = (n_use + HIT_THREADS - 1) / HIT_THREADS;
+    for (int64_t r = 0; r < rounds; ++r) {
+        const int64_t j = r * HIT_THREADS + threadIdx.x;
+        const bool live = j < n_use;
+        uint64_t xlo = 0, xhi = 0, dlo = 0, dhi = 0;
+        double a = 0.0;
+        if (live) {
+            uint64_t hi, lo;
+            phase128_exact((uint32_t)a_frac, (uint32_t)(a_frac >> 32), (uint32_t)a_int, (uint32_t)(a_int >> 32),
+                           t.g0[j], t.g1[j], t.g2[j], t.g3[j], t.g4[j], hi, lo);
+            const uint64_t plo = lo, phi = hi + t.psi[j];
+            phase128_exact((uint32_t)sf, (uint32_t)(sf >> 32), (uint32_t)si, (uint32_t)(si >> 32), t.g0[j], t.g1[j],
+                           t.g2[j], t.g3[j], t.g4[j], dhi, dlo);
+            uint64_t mlo = (uint64_t)mabs * dlo;
+            uint64_t mhi = __umul64hi((uint64_t)mabs, dlo) + (uint64_t)mabs * dhi;
+            if (m0 < 0) {
+                mlo = ~mlo + 1;
+                mhi = ~mhi + (mlo == 0 ? 1 : 0);
+            }
+            xlo = plo + mlo;
+            xhi = phi + mhi + (xlo < mlo ? 1 : 0);
+            const double g = t.gamma[j];
+            a = 2.0 * t.alpha[j] * exp(-k * g * g);
+        }
+        for (int m = 0; m < n_m; ++m) {
+            double v = 0.0;
+            if (live) {
+                double sn, cs;
+                sincos_turns_quad(s64_turns_to_f64(xhi), sn, cs);
+                v = a * cs;
+                const uint64_t nlo = xlo + dlo;
+                xhi = xhi + dhi + (nlo < xlo ? 1 : 0);
+                xlo = nlo;
+            }
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) acc[warp * n_m + m] += v;
+        }
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < n_m; m += HIT_THREADS) {
+        double s = 0.0;
+        for (int w = 0; w < HIT_THREADS / 32; ++w) s += acc[w * n_m + m];
+        out_h[(int64_t)p * n_m + m] = s;
+    }
+}
+
 __global__ void scan_reduce_kernel(const double *partial, int P, int n_chunk, int n_m, double *h) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)P * n_m) return;
@@ -145,6 +208,36 @@ extern "C" int mb_grid_scan(mb_table *h, int64_t P, const uint64_t *v_int, const
     }
     const int64_t total = P * n_m;
     scan_reduce_kernel<<<(unsigned)((total + 255) / 256), 256, 0, t.stream>>>(partial, (int)P, (int)n_chunk, (int)n_m, d_h);
+    MB_CUDA(cudaGetLastError());
+    MB_CUDA(cudaMemcpyAsync(out_h, d_h, hb, cudaMemcpyDeviceToHost, t.stream));
+    MB_CUDA(cudaStreamSynchronize(t.stream));
+    return MB_OK;
+}
+
+extern "C" int mb_hit_scan(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k,
+                           int64_t n_use, uint64_t step_int, uint64_t step_frac, int64_t m0, int64_t n_m,
+                           double *out_h) {
+    MB_CHECK_ARG(h && v_int && v_frac && out_h, "mb_hit_scan: null argument");
+    MB_CHECK_ARG(P >= 0 && P <= (1 << 24), "mb_hit_scan: P=%lld", (long long)P);
+    MB_CHECK_ARG(n_m >= 1 && n_m <= HIT_MAX_M, "mb_hit_scan: n_m=%lld (1..%d)", (long long)n_m, HIT_MAX_M);
+    MB_CHECK_ARG(m0 > -((int64_t)1 << 31) && m0 + n_m < ((int64_t)1 << 31), "mb_hit_scan: grid indices exceed 2^31");
+    MB_CHECK_ARG(std::isfinite(k) && k >= 0.0, "mb_hit_scan: k=%g", k);
+    if (P == 0) return MB_OK;
+    Table &t = table_of(h);
+    MB_CHECK_ARG(n_use >= 0 && n_use <= t.n, "mb_hit_scan: n_use=%lld of %lld", (long long)n_use, (long long)t.n);
+    MB_TRY(device_guard(t.device));
+    const size_t cb = (size_t)P * 8, hb = (size_t)P * n_m * 8;
+    MB_TRY(t.io.ensure(2 * cb + hb + 256));
+    char *base = (char *)t.io.p;
+    uint64_t *d_vi = (uint64_t *)base, *d_vf = (uint64_t *)(base + cb);
+    double *d_h = (double *)(base + ((2 * cb + 255) & ~(size_t)255));
+    MB_CUDA(cudaMemcpyAsync(d_vi, v_int, cb, cudaMemcpyHostToDevice, t.stream));
+    MB_CUDA(cudaMemcpyAsync(d_vf, v_frac, cb, cudaMemcpyHostToDevice, t.stream));
+    const size_t smem = (size_t)(HIT_THREADS / 32) * n_m * sizeof(double);
+    if (smem > 48 * 1024)
+        MB_CUDA(cudaFuncSetAttribute(k2_hit_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k2_hit_scan_kernel<<<(unsigned)P, HIT_THREADS, smem, t.stream>>>(view(t), d_vi, d_vf, step_int, step_frac, m0,
+                                                                      (int)n_m, n_use, k, d_h);
     MB_CUDA(cudaGetLastError());
     MB_CUDA(cudaMemcpyAsync(out_h, d_h, hb, cudaMemcpyDeviceToHost, t.stream));
     MB_CUDA(cudaStreamSynchronize(t.stream));

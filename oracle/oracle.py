@@ -189,6 +189,49 @@ def reference_candidates(cands):
     return x_lo, x_hi, dy0
 
 
+# ------------------------------------------------------------------ ZeroData::polish restated
+
+def zerodata_polish(top, two_astar, gamma, thresholds=(0.895, 0.918, 0.948)):
+    """search/gpu_mertens_stream.cu:381-505 for one hit, in FP64 numpy: top = the signed top word
+    of ph = xh ghi + xl glo - psi (int64 per zero), angle = top pi/2^63; five grid stages with
+    early exits.  Returns (best_h, best_dy)."""
+    SCALE = np.pi / 9223372036854775808.0
+    ang = top.astype(np.float64) * SCALE
+    g = np.asarray(gamma, np.float64)
+    ta = np.asarray(two_astar, np.float64)
+    n = len(g)
+
+    def grid(K, m_half, step, centre, base_ang):
+        dys = centre + np.arange(-m_half, m_half + 1) * step
+        A = ta[:K] * np.cos(base_ang[:K])
+        B = ta[:K] * np.sin(base_ang[:K])
+        th = g[None, :K] * (dys - centre)[:, None]
+        s = (A[None, :] * np.cos(th) - B[None, :] * np.sin(th)).sum(axis=1)
+        j = int(np.argmax(np.abs(s)))
+        return float(s[j]), float(dys[j]), float(abs(s[j]))
+
+    best_h, best_dy, b = grid(256, 38, 1.5e-4, 0.0, ang)
+    if thresholds[0] is not None and b < thresholds[0]:
+        return best_h, best_dy
+    best_h, best_dy, b = grid(512, 228, 2.5e-5, 0.0, ang)
+    if thresholds[1] is not None and b < thresholds[1]:
+        return best_h, best_dy
+    centre = best_dy
+    best_h, best_dy, b = grid(2048, 60, 1e-5, centre, ang + g * centre)
+    if thresholds[2] is not None and b < thresholds[2]:
+        return best_h, best_dy
+    centre = best_dy
+    K2 = min(15000, n)
+    dys = centre + np.arange(-320, 321) * 2.5e-6
+    s = np.array([(ta[:K2] * np.cos(ang[:K2] + g[:K2] * dy)).sum() for dy in dys])
+    best_dy = float(dys[int(np.argmax(np.abs(s)))])
+    centre = best_dy
+    dys = centre + np.arange(-120, 121) * 5e-7
+    s = np.array([(ta * np.cos(ang + g * dy)).sum() for dy in dys])
+    j = int(np.argmax(np.abs(s)))
+    return float(s[j]), float(dys[j])
+
+
 # ------------------------------------------------------------------ reference evaluator
 
 class RefLib:

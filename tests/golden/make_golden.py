@@ -1,0 +1,148 @@
+"""Generates the golden fixtures in this directory (run once; the outputs are committed).
+
+    python tests/golden/make_golden.py [--skip-full-ball]
+
+small_plain.json    64 candidates x 10,000 synthetic zeros (table seed 1, candidate seed 2),
+                    k = 3e-9, T = inf:
+                      * the reference's own compiled evaluator (oracle/_ref/libpath1_eval.so from
+                        search/path1_eval_fast.cpp): compute_peak_AB + h0 = sum w A
+                        (polish_peaks_with_weights with grid_steps = 0) and its polished h/ddy with
+                        the drivers' settings (grid_half_width 2.5e-4, 40 steps);
+                      * the binary128 oracle's K2, dK2/ddelta, dK2/dk (hi + lo doubles);
+                      * mpmath interval balls of K2 for 4 candidates (220 bits);
+                      * exact phases floor(frac(v G) 2^128) for 16 (candidate, zero) pairs.
+peak2_full_ball.json the interval ball of K2 at the reference's Peak2 point over all 2,325,572
+                    synthetic zeros below 1.3e6 (table seed 1), k = 1.5e-10, as exact rational
+                    endpoints (mpmath iv at 220 bits, summed in 64 worker processes' chunks),
+                    plus the binary128 value.
+Each fixture records the SHA-256 of the table arrays so a generator change is detected.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import math
+import os
+import sys
+import time
+from fractions import Fraction
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from mertens_bound_b200 import synth  # noqa: E402
+
+
+def table_sha(t) -> str:
+    h = hashlib.sha256()
+    for a in (t.G3, t.gamma, t.c_re, t.c_im):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def frac_str(q: Fraction) -> str:
+    return f"{q.numerator}/{q.denominator}"
+
+
+def small_fixture():
+    from oracle.interval import bounds, k2_ball
+    from oracle.oracle import Oracle, RefLib, phase128_bigint, reference_candidates, reference_format
+
+    t = synth.make_table(10_000, seed=1)
+    c = synth.make_candidates(64, seed=2)
+    k = 3e-9
+    O = Oracle()
+    hi, lo = O.k2(c, t, k, t.n)
+    out = {"table": {"n": t.n, "seed": 1, "sha256": table_sha(t)}, "candidates": {"seed": 2, "P": 64},
+           "k": k, "T": "inf",
+           "v_int": [str(int(x)) for x in c.v_int], "v_frac": [str(int(x)) for x in c.v_frac],
+           "oracle_k2": {"val": [[float(hi[p, 0]), float(lo[p, 0])] for p in range(64)],
+                         "dd": [[float(hi[p, 1]), float(lo[p, 1])] for p in range(64)],
+                         "dk": [[float(hi[p, 2]), float(lo[p, 2])] for p in range(64)]}}
+    if RefLib.available():
+        R = RefLib()
+        A, B = R.peak_AB(reference_candidates(c), reference_format(t))
+        w = np.exp(-k * t.gamma ** 2)
+        h0, _, _ = R.polish(A, B, t.gamma, w, 2.5e-4, 0)
+        hu, hp, dp = R.polish(A, B, t.gamma, w, 2.5e-4, 40)
+        out["reference_evaluator"] = {"h0": [float(x) for x in h0], "h_pol": [float(x) for x in hp],
+                                      "ddy_pol": [float(x) for x in dp],
+                                      "source": "search/path1_eval_fast.cpp compiled by oracle/Makefile"}
+    balls = []
+    for p in range(4):
+        val, _, _ = k2_ball(c.v_int[p], c.v_frac[p], 0.0, t.G3, t.c_re, t.c_im, k, t.n)
+        a, b = bounds(val)
+        balls.append([frac_str(a), frac_str(b)])
+    out["interval_balls_first4"] = balls
+    pairs = []
+    rng = np.random.default_rng(7)
+    for _ in range(16):
+        p, j = int(rng.integers(64)), int(rng.integers(t.n))
+        h, l = phase128_bigint(c.v_int[p], c.v_frac[p], t.G3[j])
+        pairs.append({"p": p, "j": j, "hi": str(h), "lo": str(l)})
+    out["exact_phases"] = pairs
+    return out
+
+
+_WORKER = {}
+
+
+def _init_worker():
+    sys.path.insert(0, ROOT)
+    from mertens_bound_b200 import synth as S
+    _WORKER["t"] = S.make_table(2_325_572, seed=1)
+    _WORKER["c"] = S.peak2_candidate()
+
+
+def _ball_chunk(args):
+    from oracle.interval import bounds, k2_ball
+    j0, j1 = args
+    t, c = _WORKER["t"], _WORKER["c"]
+    val, _, _ = k2_ball(c.v_int[0], c.v_frac[0], 0.0, t.G3[j0:j1], t.c_re[j0:j1], t.c_im[j0:j1], 1.5e-10, j1 - j0)
+    a, b = bounds(val)
+    return j0, frac_str(a), frac_str(b)
+
+
+def full_ball_fixture(workers: int):
+    import multiprocessing as mp
+    from oracle.oracle import Oracle
+
+    t = synth.make_table(2_325_572, seed=1)
+    c = synth.peak2_candidate()
+    n = t.n
+    edges = np.linspace(0, n, 513).astype(int)
+    tasks = [(int(a), int(b)) for a, b in zip(edges[:-1], edges[1:])]
+    t0 = time.time()
+    with mp.get_context("spawn").Pool(workers, initializer=_init_worker) as pool:
+        parts = pool.map(_ball_chunk, tasks, chunksize=1)
+    lo = sum((Fraction(a) for _, a, _ in parts), Fraction(0))
+    hi = sum((Fraction(b) for _, _, b in parts), Fraction(0))
+    qhi, qlo = Oracle().k2(c, t, 1.5e-10, n)
+    return {"table": {"n": n, "seed": 1, "sha256": table_sha(t)}, "v": synth.PEAK2_STR,
+            "v_int": str(int(c.v_int[0])), "v_frac": str(int(c.v_frac[0])), "k": 1.5e-10, "T0": 1.3e6,
+            "ball_lo": frac_str(lo), "ball_hi": frac_str(hi), "ball_width": float(hi - lo),
+            "oracle_k2": [float(qhi[0, 0]), float(qlo[0, 0])],
+            "method": "mpmath iv at 220 bits per term over 512 zero ranges, exact rational sum",
+            "seconds": round(time.time() - t0, 1)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--skip-full-ball", action="store_true")
+    ap.add_argument("--workers", type=int, default=os.cpu_count())
+    a = ap.parse_args()
+    with open(os.path.join(HERE, "small_plain.json"), "w") as f:
+        json.dump(small_fixture(), f, indent=1)
+    print("wrote small_plain.json", flush=True)
+    if not a.skip_full_ball:
+        with open(os.path.join(HERE, "peak2_full_ball.json"), "w") as f:
+            json.dump(full_ball_fixture(a.workers), f, indent=1)
+        print("wrote peak2_full_ball.json", flush=True)
+
+
+if __name__ == "__main__":
+    main()
