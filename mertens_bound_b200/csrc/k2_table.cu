@@ -102,11 +102,9 @@ extern "C" int mb_table_create(const uint64_t *G3, const double *c_re, const dou
     MB_CHECK_ARG(G3 && c_re && c_im && gamma, "mb_table_create: null array");
     MB_CHECK_ARG(n >= 1 && n <= ((int64_t)1 << 31), "mb_table_create: n=%lld out of range",
                  (long long)n);
-    int ndev = 0;
-    MB_CUDA(cudaGetDeviceCount(&ndev));
-    MB_CHECK_ARG(device >= 0 && device < ndev, "mb_table_create: device %d of %d", device, ndev);
+    MB_CHECK_ARG(device >= 0, "mb_table_create: device %d", device);
 
-    // ---- validation (host, O(n))
+    // ---- validation (host, O(n)), before any CUDA call
     const long double two_pi = 6.28318530717958647692528676655900577L;
     for (int64_t j = 0; j < n; ++j) {
         double g = gamma[j];
@@ -136,6 +134,9 @@ extern "C" int mb_table_create(const uint64_t *G3, const double *c_re, const dou
         }
     }
 
+    int ndev = 0;
+    MB_CUDA(cudaGetDeviceCount(&ndev));
+    MB_CHECK_ARG(device < ndev, "mb_table_create: device %d of %d", device, ndev);
     MB_TRY(device_guard(device));
     mb_table *h = new mb_table();
     Table &t = h->t;
