@@ -131,6 +131,16 @@ typedef struct mb_plan mb_plan;
 
 int mb_plan_create(mb_table *t, int n_groups, const int64_t *counts, const double *ks,
                    const double *Ts, double tol, mb_plan **out);
+/* Register a per-zero weight vector w[n] (n = table size) with the table; *slot names it.
+ * The search drivers score the same candidates under several weights besides the Gaussians:
+ * the Jurkat-Peyerimhoff kernel, raw (w = 1) and a first-10k cutoff
+ * (search/eval_tech1_600k.py:243-249). */
+int mb_table_add_weights(mb_table *t, const double *w, int64_t n, int *slot);
+/* As mb_plan_create, with weight_slots[g] = a registered weight vector for group g, or -1 for
+ * exp(-k_g gamma^2).  For a weight vector, dk returns -2 sum gamma^2 w Re(c e^{i gamma v}) =
+ * d2K/ddelta2 (the Newton denominator); k_g is ignored. */
+int mb_plan_create_weighted(mb_table *t, int n_groups, const int64_t *counts, const double *ks, const double *Ts,
+                            const int *weight_slots, double tol, mb_plan **out);
 int mb_plan_destroy(mb_plan *p);
 /* Override the tile shape of group g: cpt in {1,2,4} candidates per thread, nzw in {1,2,4,8}
  * warps splitting the zeros, chunk sizes in zeros (0 = automatic; multiples of 128 / 256). */
@@ -195,6 +205,45 @@ int mb_grid_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *
  * 256, 512, 2048, 15000 and all zeros at decreasing steps) are calls of this. */
 int mb_hit_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k, int64_t n_use,
                 uint64_t step_int, uint64_t step_frac, int64_t m0, int64_t n_m, double *out_h);
+
+/* ---- per-peak polish contracts of search/path1_kernel_opt.py ------------------------------
+ * A_j, B_j = 2 Re, 2 Im of c_j e^{i gamma_j y} and h(ddy) = sum_j w_j (A_j cos(gamma_j ddy) -
+ * B_j sin(gamma_j ddy)).  Matrices are row-major (n_peaks, n_zeros) host arrays. */
+
+/* out_A/out_B (P x n_zeros) at y = v + delta from the exact 128-bit phase; angle error below
+ * 2 pi (|delta| 2^-52 + 2^-100), so A, B carry only FP64 sincos and product rounding.
+ * |delta| <= 2^16.  Replaces compute_exact_mpfr_AB (search/path1_kernel_opt.py:71-91: one y,
+ * 256-bit mpfr phase, rounded to FP64). */
+int mb_exact_AB(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
+                int64_t n_zeros, double *out_A, double *out_B);
+
+/* polish_single_peak (search/path1_kernel_opt.py:94-147) for each of n_peaks rows (row stride ld,
+ * first n_zeros columns used): h0 = sum w A; grid ddy = numpy.linspace(-grid_hw, grid_hw,
+ * 2 grid_steps + 1) over all n_zeros (none if grid_steps = 0), first argmax of |h|; Newton
+ * (8 steps, clamp 2e-5, stop below 1e-14 or |h''| <= 1e-12) from 0 and from the grid's best;
+ * a start's h is kept only if |h| > the best so far (which starts at h0, ddy 0). */
+int mb_polish_single_peak(int64_t n_peaks, int64_t n_zeros, int64_t ld, const double *A, const double *B,
+                          const double *gamma, const double *w, double grid_hw, int grid_steps,
+                          double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);
+
+/* fast_polish_batch_blas (search/path1_kernel_opt.py:150-221): degree-16 Taylor moments of h in
+ * u = gamma 1e-4 around ddy = 0 evaluated on ddy_grid (first argmax of |h|), h_unpol = the
+ * zeroth moment; then exact Newton (4 steps, clamp 1e-5, stop below 1e-13) from the grid point
+ * on the `top` peaks of largest |h_pol| (the reference uses 25; equal |h| in index order): a
+ * peak keeps (h, ddy) if |h| > |h_unpol|, else (h_unpol, 0). */
+int mb_fast_polish_batch(int64_t n_peaks, int64_t n_zeros, const double *A, const double *B, const double *gamma,
+                         const double *w, const double *ddy_grid, int64_t n_grid, int top, double *out_h_unpol,
+                         double *out_h_pol, double *out_ddy_pol);
+
+/* The two polishes with (A_j, B_j) of peak p computed on the fly at y = v_p + delta_p as in
+ * mb_exact_AB (no P x N matrices), over the table's first n_zeros zeros, gamma = the table's
+ * FP64 gamma and w = a weight vector registered by mb_table_add_weights. */
+int mb_polish_single_exact(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                           const double *delta, int64_t n_zeros, int weight_slot, double grid_hw, int grid_steps,
+                           double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);
+int mb_fast_polish_exact(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                         const double *delta, int64_t n_zeros, int weight_slot, const double *ddy_grid,
+                         int64_t n_grid, int top, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);
 
 /* ---- compatibility with the reference's libpath1_eval.so ---------------------------------
  * Same names, signatures and host-array contracts as search/path1_eval_fast.cpp:15 and :58, so

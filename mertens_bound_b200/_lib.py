@@ -33,6 +33,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_k2_plain_dev": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
     "mb_plan_create": (i32, [vp, i32, vp, vp, vp, f64, C.POINTER(vp)]),
     "mb_plan_destroy": (i32, [vp]),
+    "mb_table_add_weights": (i32, [vp, vp, i64, C.POINTER(i32)]),
+    "mb_plan_create_weighted": (i32, [vp, i32, vp, vp, vp, vp, f64, C.POINTER(vp)]),
     "mb_plan_set_shape": (i32, [vp, i32, i32, i32, i64, i64]),
     "mb_plan_info": (i32, [vp, i64p, f64p, C.POINTER(i32)]),
     "mb_plan_configure": (i32, [vp, i32, i32, f64]),
@@ -51,6 +53,11 @@ SIGNATURES: dict[str, tuple] = {
     "mb_k2_certified_range": (i32, [vp, i64, vp, vp, vp, f64, f64, i64, i64, vp, vp, vp, vp]),
     "mb_grid_scan": (i32, [vp, i64, vp, vp, f64, f64, C.c_uint64, C.c_uint64, i64, i64, vp]),
     "mb_hit_scan": (i32, [vp, i64, vp, vp, f64, i64, C.c_uint64, C.c_uint64, i64, i64, vp]),
+    "mb_exact_AB": (i32, [vp, i64, vp, vp, vp, i64, vp, vp]),
+    "mb_polish_single_peak": (i32, [i64, i64, i64, vp, vp, vp, vp, f64, i32, vp, vp, vp]),
+    "mb_fast_polish_batch": (i32, [i64, i64, vp, vp, vp, vp, vp, i64, i32, vp, vp, vp]),
+    "mb_polish_single_exact": (i32, [vp, i64, vp, vp, vp, i64, i32, f64, i32, vp, vp, vp]),
+    "mb_fast_polish_exact": (i32, [vp, i64, vp, vp, vp, i64, i32, vp, i64, i32, vp, vp, vp]),
     "compute_peak_AB": (None, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "polish_peaks_with_weights": (None, [i32, i32, vp, vp, vp, vp, f64, i32, vp, vp, vp]),
     "mb_compute_peak_AB": (i32, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),

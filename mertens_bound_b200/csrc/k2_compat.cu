@@ -18,6 +18,7 @@
 #include <mutex>
 
 #include "k2_internal.h"
+#include "k2_polish.cuh"
 
 namespace mb {
 namespace {
@@ -61,113 +62,26 @@ __global__ void peak_AB_kernel(int n_peaks, int n_zeros, const uint64_t *x_lo, c
     B[o] = ta * s;
 }
 
-constexpr int POLISH_THREADS = 256;
+}  // namespace
 
-__device__ double block_sum(double x, double *red) {
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __syncthreads();
-    if (lane == 0) red[warp] = x;
-    __syncthreads();
-    double s = 0.0;
-    for (int w = 0; w < POLISH_THREADS / 32; ++w) s += red[w];
-    return s;
-}
-
-// One CTA per peak; the sequential steps of the reference loop are block-wide reductions.
-__global__ void __launch_bounds__(POLISH_THREADS)
-polish_kernel(int n_zeros, const double *A, const double *B, const double *gamma, const double *w,
-              double half, int steps, double *h_unpol, double *h_pol, double *ddy_pol) {
-    __shared__ double red[POLISH_THREADS / 32];
-    const int p = blockIdx.x;
-    const double *Ap = A + (size_t)p * n_zeros, *Bp = B + (size_t)p * n_zeros;
-    double s = 0.0;
-    for (int i = threadIdx.x; i < n_zeros; i += POLISH_THREADS) s += w[i] * Ap[i];
-    const double h0 = block_sum(s, red);
-    double best_ddy = 0.0, best_abs = fabs(h0);
-    const int k_scan = n_zeros < 4096 ? n_zeros : 4096;
-    if (steps > 0) {
-        for (int m = -steps; m <= steps; ++m) {
-            const double ddy = (half * m) / steps;
-            double hs = 0.0;
-            for (int i = threadIdx.x; i < k_scan; i += POLISH_THREADS) {
-                double sn, cs;
-                sincos(gamma[i] * ddy, &sn, &cs);
-                hs += w[i] * (Ap[i] * cs - Bp[i] * sn);
-            }
-            hs = block_sum(hs, red);
-            if (fabs(hs) > best_abs) {
-                best_abs = fabs(hs);
-                best_ddy = ddy;
-            }
-        }
-    }
-    double ddy = best_ddy;
-    for (int it = 0; it < 6; ++it) {
-        double fp = 0.0, fpp = 0.0;
-        for (int i = threadIdx.x; i < n_zeros; i += POLISH_THREADS) {
-            const double g = gamma[i];
-            double sn, cs;
-            sincos(g * ddy, &sn, &cs);
-            const double val = Ap[i] * cs - Bp[i] * sn;
-            const double dval = g * (-Ap[i] * sn - Bp[i] * cs);
-            fp += w[i] * dval;
-            fpp += w[i] * (-g * g * val);
-        }
-        fp = block_sum(fp, red);
-        fpp = block_sum(fpp, red);
-        if (fabs(fpp) > 1e-12) {
-            double step = fp / fpp;
-            step = fmin(fmax(step, -1e-4), 1e-4);
-            ddy -= step;
-            if (fabs(step) < 1e-13) break;
-        } else {
-            break;
-        }
-    }
-    double hf = 0.0;
-    for (int i = threadIdx.x; i < n_zeros; i += POLISH_THREADS) {
-        double sn, cs;
-        sincos(gamma[i] * ddy, &sn, &cs);
-        hf += w[i] * (Ap[i] * cs - Bp[i] * sn);
-    }
-    hf = block_sum(hf, red);
-    if (threadIdx.x == 0) {
-        h_unpol[p] = h0;
-        if (fabs(h0) > fabs(hf)) {
-            h_pol[p] = h0;
-            ddy_pol[p] = 0.0;
-        } else {
-            h_pol[p] = hf;
-            ddy_pol[p] = ddy;
-        }
-    }
-}
-
-// Per-device grow-only buffers of the compatibility calls (the reference API has no handle).
-struct CompatState {
+// Per-device grow-only buffers of the handle-free entry points (the reference API has no handle).
+struct ScratchState {
     std::mutex mu;
     DevBuf buf[64];
 };
-CompatState g_compat;
+static ScratchState g_scratch;
 
-int compat_buffer(size_t bytes, void **out) {
+std::mutex &scratch_mutex() { return g_scratch.mu; }
+
+int scratch_buffer(size_t bytes, void **out) {
     int dev = 0;
     MB_CUDA(cudaGetDevice(&dev));
-    MB_CHECK_ARG(dev >= 0 && dev < 64, "compat: device %d", dev);
-    MB_TRY(g_compat.buf[dev].ensure(bytes));
-    *out = g_compat.buf[dev].p;
+    MB_CHECK_ARG(dev >= 0 && dev < 64, "scratch: device %d", dev);
+    MB_TRY(g_scratch.buf[dev].ensure(bytes));
+    *out = g_scratch.buf[dev].p;
     return MB_OK;
 }
 
-template <typename T>
-T *carve(char *&p, size_t n) {
-    T *r = (T *)p;
-    p += ((n * sizeof(T) + 255) / 256) * 256;
-    return r;
-}
-
-}  // namespace
 }  // namespace mb
 
 using namespace mb;
@@ -181,13 +95,13 @@ extern "C" int mb_compute_peak_AB(int n_peaks, const uint64_t *x_lo_arr, const u
     if (n_peaks == 0 || n_zeros == 0) return MB_OK;
     MB_CHECK_ARG(x_lo_arr && x_hi_arr && dy0_arr && alpha && gamma && ghi_lo && ghi_hi && glo_lo && glo_hi &&
                  psi_lo && psi_hi && out_A && out_B, "compute_peak_AB: null array");
-    std::lock_guard<std::mutex> lock(g_compat.mu);
+    std::lock_guard<std::mutex> lock(scratch_mutex());
     const size_t N = (size_t)n_zeros;
     // peaks per pass so that the A/B slabs stay within 2 GiB of device memory
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n_peaks, ((size_t)1 << 31) / (16 * N)));
     const size_t bytes = 8 * (N * 8 + 256) + 3 * ((size_t)chunk * 8 + 256) + 2 * ((size_t)chunk * N * 8 + 256);
     void *base = nullptr;
-    MB_TRY(compat_buffer(bytes, &base));
+    MB_TRY(scratch_buffer(bytes, &base));
     char *p = (char *)base;
     double *d_alpha = carve<double>(p, N), *d_gamma = carve<double>(p, N);
     uint64_t *d_ghl = carve<uint64_t>(p, N), *d_ghh = carve<uint64_t>(p, N), *d_gll = carve<uint64_t>(p, N),
@@ -229,12 +143,12 @@ extern "C" int mb_polish_peaks_with_weights(int n_peaks, int n_zeros, const doub
     MB_CHECK_ARG(A && B && gamma && w && out_h_unpol && out_h_pol && out_ddy_pol,
                  "polish_peaks_with_weights: null array");
     MB_CHECK_ARG(std::isfinite(grid_half_width), "polish_peaks_with_weights: grid_half_width is not finite");
-    std::lock_guard<std::mutex> lock(g_compat.mu);
+    std::lock_guard<std::mutex> lock(scratch_mutex());
     const size_t N = (size_t)std::max(n_zeros, 1);
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n_peaks, ((size_t)1 << 31) / (16 * N)));
     const size_t bytes = 2 * (N * 8 + 256) + 2 * ((size_t)chunk * N * 8 + 256) + 3 * ((size_t)chunk * 8 + 256);
     void *base = nullptr;
-    MB_TRY(compat_buffer(bytes, &base));
+    MB_TRY(scratch_buffer(bytes, &base));
     char *p = (char *)base;
     double *d_g = carve<double>(p, N), *d_w = carve<double>(p, N);
     double *d_A = carve<double>(p, (size_t)chunk * N), *d_B = carve<double>(p, (size_t)chunk * N);
@@ -250,8 +164,8 @@ extern "C" int mb_polish_peaks_with_weights(int n_peaks, int n_zeros, const doub
             MB_CUDA(cudaMemcpyAsync(d_A, A + (size_t)p0 * n_zeros, (size_t)np * n_zeros * 8, cudaMemcpyHostToDevice, s));
             MB_CUDA(cudaMemcpyAsync(d_B, B + (size_t)p0 * n_zeros, (size_t)np * n_zeros * 8, cudaMemcpyHostToDevice, s));
         }
-        polish_kernel<<<np, POLISH_THREADS, 0, s>>>(n_zeros, d_A, d_B, d_g, d_w, grid_half_width, grid_steps, d_hu,
-                                                    d_hp, d_dp);
+        PolishArgs a{n_zeros, d_g, d_w, nullptr, grid_steps, grid_half_width, nullptr, d_hu, d_hp, d_dp};
+        peak_polish_kernel<ABMatrix, POLISH_EVAL_FAST><<<np, POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, a);
         MB_CUDA(cudaGetLastError());
         MB_CUDA(cudaMemcpyAsync(out_h_unpol + p0, d_hu, np * 8, cudaMemcpyDeviceToHost, s));
         MB_CUDA(cudaMemcpyAsync(out_h_pol + p0, d_hp, np * 8, cudaMemcpyDeviceToHost, s));

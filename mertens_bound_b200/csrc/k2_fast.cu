@@ -151,10 +151,11 @@ MB_DEV void heavy_tile(const ZHeavy *tile, int nt, int zl, int ZL, const CandReg
     }
 }
 
-// Stage one zero into a tile record (one thread per zero).
-MB_DEV void stage_light(const TabView &t, int64_t j, double k, ZLight &r) {
+// Stage one zero into a tile record (one thread per zero).  The weight is exp(-k gamma^2), or
+// w[j] when the group carries its own weight vector.
+MB_DEV void stage_light(const TabView &t, int64_t j, double k, const double *w, ZLight &r) {
     double g = t.gamma[j];
-    double a = 2.0 * t.alpha[j] * exp(-k * g * g);
+    double a = 2.0 * t.alpha[j] * (w ? w[j] : exp(-k * g * g));
     uint32_t b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j], c1 = t.g1[j];
     r.b0 = b0; r.b1 = b1; r.gi = gi;
     r.psi32 = (uint32_t)((t.psi[j] + 0x80000000ull) >> 32) + 2u;
@@ -168,9 +169,9 @@ MB_DEV void stage_light(const TabView &t, int64_t j, double k, ZLight &r) {
     r.pad = 0.f;
 }
 
-MB_DEV void stage_heavy(const TabView &t, int64_t j, double k, ZHeavy &r) {
+MB_DEV void stage_heavy(const TabView &t, int64_t j, double k, const double *w, ZHeavy &r) {
     double g = t.gamma[j];
-    double a = 2.0 * t.alpha[j] * exp(-k * g * g);
+    double a = 2.0 * t.alpha[j] * (w ? w[j] : exp(-k * g * g));
     uint32_t c0 = t.g0[j], c1 = t.g1[j], b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j];
     r.b0 = b0; r.b1 = b1; r.gi = gi; r.pad = 0;
     r.b0s = u32_to_f64(b0) * TWO_M64;
@@ -240,7 +241,7 @@ MB_DEV void light_item(const FastItem &it, const FastGroup &gr, const TabView &t
     for (int64_t tb = it.z0; tb < it.z1; tb += LIGHT_TILE) {
         __syncthreads();
         int64_t j = tb + threadIdx.x;
-        if (threadIdx.x < LIGHT_TILE && j < it.z1) stage_light(t, j, gr.k, tile[threadIdx.x]);
+        if (threadIdx.x < LIGHT_TILE && j < it.z1) stage_light(t, j, gr.k, gr.w, tile[threadIdx.x]);
         __syncthreads();
         light_tile<CPT>(tile, (int)min((int64_t)LIGHT_TILE, it.z1 - tb), zw, nzw, cr, hi, lo);
     }
@@ -270,7 +271,7 @@ MB_DEV void heavy_item(const FastItem &it, const FastGroup &gr, const TabView &t
     for (int64_t tb = it.z0; tb < it.z1; tb += HEAVY_TILE) {
         __syncthreads();
         int64_t j = tb + threadIdx.x;
-        if (threadIdx.x < HEAVY_TILE && j < it.z1) stage_heavy(t, j, gr.k, tile[threadIdx.x]);
+        if (threadIdx.x < HEAVY_TILE && j < it.z1) stage_heavy(t, j, gr.k, gr.w, tile[threadIdx.x]);
         __syncthreads();
         heavy_tile<CPT>(tile, (int)min((int64_t)HEAVY_TILE, it.z1 - tb), zw, nzw, cr, res);
     }

@@ -14,6 +14,7 @@ struct FastGroup {
     int64_t pbase;     // offset (in doubles) of this group's partial sums
     int n_chunks;      // zero chunks (heavy then light); partial[pbase + (chunk*nc + p-c0)*3 + q]
     int pad;
+    const double *w;   // per-zero weights (device) replacing exp(-k gamma^2), or null
 };
 
 // One work item: a candidate tile of one group against one zero chunk of one tier.

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -61,6 +62,9 @@ struct Table {
     uint64_t *d_psi = nullptr;
     std::vector<double> h_gamma;      // host copies for cutoffs and error planning
     std::vector<double> h_alpha;
+    // per-zero weight vectors registered with the table (device copies + host copies)
+    std::vector<double *> d_weights;
+    std::vector<std::vector<double>> h_weights;
     cudaStream_t stream = nullptr;    // the library's own stream for host-pointer calls
     cudaStream_t side = nullptr;      // second stream: heavy tier beside the light tier
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -89,6 +93,19 @@ struct CandView {
 };
 
 int device_guard(int device);
+
+// Per-device grow-only scratch of the handle-free entry points (reference-compatible calls);
+// hold scratch_mutex() while using it.
+std::mutex &scratch_mutex();
+int scratch_buffer(size_t bytes, void **out);
+
+// Bump allocation of 256-byte aligned sub-arrays from a scratch block.
+template <typename T>
+T *carve(char *&p, size_t n) {
+    T *r = (T *)p;
+    p += ((n * sizeof(T) + 255) / 256) * 256;
+    return r;
+}
 
 // Kernel launchers (return MB_OK or an MB_ERR_* code).
 Table &table_of(struct ::mb_table *h);

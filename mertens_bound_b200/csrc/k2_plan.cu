@@ -18,6 +18,7 @@ struct mb_plan {
     double tol = 1e-10;
     std::vector<int64_t> counts;
     std::vector<double> ks, Ts;
+    std::vector<int> wslot;        // per group: table weight vector, or -1 for exp(-k gamma^2)
     std::vector<FastGroup> groups;
     std::vector<FastItem> items;
     std::vector<int64_t> n_T, n_heavy;
@@ -74,13 +75,13 @@ int default_nzw(int64_t P, int cpt) {
 
 // Tier boundary: the smallest n_h with EPS_LIGHT * sum_{j>=n_h} a_j <= budget, where
 // a_j = 2|c_j| exp(-k gamma_j^2) bounds |term_j|.  Returns the bound of the whole sum.
-void plan_tiers(const Table &t, int64_t n_use, double k, double tol, int64_t &n_h, double &bound,
+void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, double tol, int64_t &n_h, double &bound,
                 double &sabs) {
     std::vector<double> a(n_use);
     double total = 0;
     for (int64_t j = 0; j < n_use; ++j) {
         double g = t.h_gamma[j];
-        a[j] = 2.0 * t.h_alpha[j] * std::exp(-k * g * g);
+        a[j] = 2.0 * t.h_alpha[j] * (wts ? std::fabs(wts[j]) : std::exp(-k * g * g));
         total += a[j];
     }
     const double budget = 0.5 * tol;
@@ -125,6 +126,7 @@ int build_items(mb_plan *p, int sms) {
         gr.c0 = c0;
         gr.nc = p->counts[g];
         gr.k = p->ks[g];
+        gr.w = p->wslot[g] >= 0 ? p->table->d_weights[p->wslot[g]] : nullptr;
         gr.pbase = pbase;
         const int nzw = p->shape_nzw[g];
         const int64_t CTh = (int64_t)(8 / nzw) * 32 * HEAVY_CPT;
@@ -240,8 +242,8 @@ int ensure_io(mb_plan *p) {
 
 }  // namespace
 
-extern "C" int mb_plan_create(mb_table *h, int n_groups, const int64_t *counts, const double *ks,
-                              const double *Ts, double tol, mb_plan **out) {
+extern "C" int mb_plan_create_weighted(mb_table *h, int n_groups, const int64_t *counts, const double *ks,
+                                       const double *Ts, const int *weight_slots, double tol, mb_plan **out) {
     MB_CHECK_ARG(out != nullptr, "mb_plan_create: out is null");
     *out = nullptr;
     MB_CHECK_ARG(h && counts && ks && Ts, "mb_plan_create: null argument");
@@ -253,6 +255,9 @@ extern "C" int mb_plan_create(mb_table *h, int n_groups, const int64_t *counts, 
         MB_CHECK_ARG(counts[g] >= 0 && counts[g] <= ((int64_t)1 << 26), "mb_plan_create: count[%d]", g);
         MB_CHECK_ARG(std::isfinite(ks[g]) && ks[g] >= 0, "mb_plan_create: k[%d]=%g", g, ks[g]);
         MB_CHECK_ARG(!std::isnan(Ts[g]), "mb_plan_create: T[%d] is NaN", g);
+        if (weight_slots)
+            MB_CHECK_ARG(weight_slots[g] >= -1 && weight_slots[g] < (int)t.d_weights.size(),
+                         "mb_plan_create: weight slot %d of group %d not registered", weight_slots[g], g);
         P += counts[g];
     }
     MB_CHECK_ARG(P <= ((int64_t)1 << 26), "mb_plan_create: total P=%lld too large", (long long)P);
@@ -272,9 +277,12 @@ extern "C" int mb_plan_create(mb_table *h, int n_groups, const int64_t *counts, 
     p->shape_nzw.resize(n_groups);
     p->heavy_chunk.assign(n_groups, 0);
     p->light_chunk.assign(n_groups, 0);
+    p->wslot.assign(n_groups, -1);
+    if (weight_slots) p->wslot.assign(weight_slots, weight_slots + n_groups);
     for (int g = 0; g < n_groups; ++g) {
         p->n_T[g] = t.count_below(Ts[g]);
-        plan_tiers(t, p->n_T[g], ks[g], tol, p->n_heavy[g], p->err_bound[g], p->sum_abs[g]);
+        const double *wh = p->wslot[g] >= 0 ? t.h_weights[p->wslot[g]].data() : nullptr;
+        plan_tiers(t, p->n_T[g], ks[g], wh, tol, p->n_heavy[g], p->err_bound[g], p->sum_abs[g]);
         p->shape_nzw[g] = default_nzw(counts[g], p->light_cpt);
     }
     int st = upload(p);
@@ -285,6 +293,11 @@ extern "C" int mb_plan_create(mb_table *h, int n_groups, const int64_t *counts, 
     }
     *out = p;
     return MB_OK;
+}
+
+extern "C" int mb_plan_create(mb_table *h, int n_groups, const int64_t *counts, const double *ks,
+                              const double *Ts, double tol, mb_plan **out) {
+    return mb_plan_create_weighted(h, n_groups, counts, ks, Ts, nullptr, tol, out);
 }
 
 extern "C" int mb_plan_destroy(mb_plan *p) {

@@ -80,6 +80,7 @@ static void free_table(Table &t) {
     cudaFree(t.d_psi);
     t.io.release();
     t.work.release();
+    for (double *w : t.d_weights) cudaFree(w);
     if (t.ev_fork) cudaEventDestroy(t.ev_fork);
     if (t.ev_join) cudaEventDestroy(t.ev_join);
     if (t.side) cudaStreamDestroy(t.side);
@@ -208,6 +209,32 @@ extern "C" int mb_table_count_below(const mb_table *h, double T, int64_t *n_out)
     MB_CHECK_ARG(h && n_out, "mb_table_count_below: null argument");
     MB_CHECK_ARG(!std::isnan(T), "mb_table_count_below: T is NaN");
     *n_out = h->t.count_below(T);
+    return MB_OK;
+}
+
+extern "C" int mb_table_add_weights(mb_table *h, const double *w, int64_t n, int *slot) {
+    MB_CHECK_ARG(h && w && slot, "mb_table_add_weights: null argument");
+    Table &t = h->t;
+    MB_CHECK_ARG(n == t.n, "mb_table_add_weights: %lld weights for a table of %lld zeros", (long long)n,
+                 (long long)t.n);
+    MB_CHECK_ARG(t.d_weights.size() < 64, "mb_table_add_weights: at most 64 weight vectors per table");
+    for (int64_t j = 0; j < n; ++j)
+        if (!std::isfinite(w[j])) {
+            set_error("mb_table_add_weights: weight %lld is not finite", (long long)j);
+            return MB_ERR_TABLE;
+        }
+    MB_TRY(device_guard(t.device));
+    double *d = nullptr;
+    MB_CUDA(cudaMalloc(&d, n * sizeof(double)));
+    cudaError_t e = cudaMemcpy(d, w, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        set_error("mb_table_add_weights: %s", cudaGetErrorString(e));
+        return MB_ERR_CUDA;
+    }
+    t.d_weights.push_back(d);
+    t.h_weights.emplace_back(w, w + n);
+    *slot = (int)t.d_weights.size() - 1;
     return MB_OK;
 }
 

@@ -55,6 +55,19 @@ class ZeroTable:
             raise ValueError("table is closed")
         return self._h
 
+    def add_weights(self, w) -> int:
+        """Register a per-zero weight vector (length n) with the table; returns its slot.
+
+        A plan group that names the slot sums 2 w_j Re(c_j e^{i gamma_j v}) instead of the
+        Gaussian exp(-k gamma_j^2) weight.
+        """
+        w = _f64(w)
+        if w.shape != (self.n,):
+            raise ValueError(f"weights must have shape ({self.n},)")
+        slot = C.c_int()
+        check(_lib.lib().mb_table_add_weights(self.handle, ptr(w), self.n, C.byref(slot)))
+        return slot.value
+
     def count_below(self, T: float) -> int:
         out = C.c_int64()
         check(_lib.lib().mb_table_count_below(self.handle, float(T), C.byref(out)))
@@ -111,18 +124,26 @@ class Plan:
     """A batched evaluation plan: groups of candidates, each at its own (k, T).
 
     counts[g] consecutive candidates form group g.  tol is the a-priori bound on |K2 error|
-    per candidate that fixes each group's heavy/light tier boundary.
+    per candidate that fixes each group's heavy/light tier boundary.  weights[g], if given, is a
+    slot from ZeroTable.add_weights (or -1 for the Gaussian exp(-k_g gamma^2)).
     """
 
-    def __init__(self, table: ZeroTable, counts, ks, Ts, tol: float = 1e-10):
+    def __init__(self, table: ZeroTable, counts, ks, Ts, tol: float = 1e-10, weights=None):
         counts = np.ascontiguousarray(counts, dtype=np.int64)
         ks = np.ascontiguousarray(ks, dtype=np.float64)
         Ts = np.ascontiguousarray(Ts, dtype=np.float64)
         if not (counts.shape == ks.shape == Ts.shape) or counts.ndim != 1:
             raise ValueError("counts, ks, Ts must be 1-D of equal length")
         h = C.c_void_p()
-        check(_lib.lib().mb_plan_create(table.handle, counts.shape[0], ptr(counts), ptr(ks), ptr(Ts),
-                                        float(tol), C.byref(h)))
+        if weights is None:
+            check(_lib.lib().mb_plan_create(table.handle, counts.shape[0], ptr(counts), ptr(ks), ptr(Ts),
+                                            float(tol), C.byref(h)))
+        else:
+            weights = np.ascontiguousarray(weights, dtype=np.int32)
+            if weights.shape != counts.shape:
+                raise ValueError("weights must name one slot per group")
+            check(_lib.lib().mb_plan_create_weighted(table.handle, counts.shape[0], ptr(counts), ptr(ks),
+                                                     ptr(Ts), ptr(weights), float(tol), C.byref(h)))
         self._h = h
         self.table = table
         self.counts, self.ks, self.Ts, self.tol = counts, ks, Ts, tol

@@ -66,13 +66,14 @@ static inline __float128 G_quad(const uint64_t *g) {
 /* K2 value and its two derivatives, in binary128.
  *   val = 2 sum w Re(c e^{i th}),  dd = dK2/ddelta = -2 sum w gam Im(c e^{i th}),
  *   dk  = dK2/dk = -2 sum w gam^2 Re(c e^{i th}),  th = 2pi frac(v G) + gam delta,
- *   w = exp(-k gam^2), gam = 2pi G (exact G, not the FP64 gamma).
+ *   w = exp(-k gam^2) (or wts[j] when wts is given: the search drivers' other weight
+ *   kernels, search/eval_tech1_600k.py:243-249), gam = 2pi G (exact G, not the FP64 gamma).
  * Zeros j < n_use are summed (the caller applies the cutoff gamma < T).
  * Each output is returned as a double pair (hi, lo) with hi + lo = the binary128 sum
  * rounded to ~106 bits, so tests can see errors far below one FP64 ulp. */
-void orc_k2_quad(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
-                 int64_t n_use, const uint64_t *G3, const double *c_re, const double *c_im,
-                 double k, double *out /* P x 6: val hi,lo, dd hi,lo, dk hi,lo */) {
+void orc_k2_quad_w(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
+                   int64_t n_use, const uint64_t *G3, const double *c_re, const double *c_im,
+                   double k, const double *wts, double *out /* P x 6: val hi,lo, dd hi,lo, dk hi,lo */) {
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t p = 0; p < P; ++p) {
         __float128 sv = 0, sd = 0, sk = 0;
@@ -86,7 +87,7 @@ void orc_k2_quad(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const
             __float128 th = Q_2PI * fr + gam * dq;
             __float128 s, c;
             sincosq(th, &s, &c);
-            __float128 w = expq(-(__float128)k * gam * gam);
+            __float128 w = wts ? (__float128)wts[j] : expq(-(__float128)k * gam * gam);
             __float128 re = (__float128)c_re[j] * c - (__float128)c_im[j] * s;
             __float128 im = (__float128)c_re[j] * s + (__float128)c_im[j] * c;
             sv += w * re;
@@ -98,6 +99,35 @@ void orc_k2_quad(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const
             double h = (double)r[i];
             out[6 * p + 2 * i] = h;
             out[6 * p + 2 * i + 1] = (double)(r[i] - (__float128)h);
+        }
+    }
+}
+
+void orc_k2_quad(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
+                 int64_t n_use, const uint64_t *G3, const double *c_re, const double *c_im,
+                 double k, double *out) {
+    orc_k2_quad_w(P, v_int, v_frac, delta, n_use, G3, c_re, c_im, k, NULL, out);
+}
+
+/* A_j = 2 Re(c_j e^{i th}), B_j = 2 Im(c_j e^{i th}) at th = 2pi frac(v G_j) + gam_j delta, in
+ * binary128 rounded to FP64: the restatement of compute_exact_mpfr_AB
+ * (search/path1_kernel_opt.py:71-91), with the exact integer phase standing in for the 256-bit
+ * mpfr product.  Output row-major (P, n_use). */
+void orc_exact_AB(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
+                  int64_t n_use, const uint64_t *G3, const double *c_re, const double *c_im, double *A,
+                  double *B) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t p = 0; p < P; ++p) {
+        __float128 dq = delta ? (__float128)delta[p] : 0;
+        for (int64_t j = 0; j < n_use; ++j) {
+            uint64_t hi, lo;
+            phase128(v_int[p], v_frac[p], G3[3 * j], G3[3 * j + 1], G3[3 * j + 2], &hi, &lo);
+            __float128 gam = Q_2PI * G_quad(&G3[3 * j]);
+            __float128 fr = ldexpq((__float128)hi, -64) + ldexpq((__float128)lo, -128);
+            __float128 s, c;
+            sincosq(Q_2PI * fr + gam * dq, &s, &c);
+            A[p * n_use + j] = (double)(2 * ((__float128)c_re[j] * c - (__float128)c_im[j] * s));
+            B[p * n_use + j] = (double)(2 * ((__float128)c_re[j] * s + (__float128)c_im[j] * c));
         }
     }
 }

@@ -12,6 +12,8 @@ Contents
                            glo = rint(G 2^98), psi = rint(((-arg c / 2pi) mod 1) 2^128), alpha = |c|;
                            x = floor(v 2^30) as u128 with the remaining fraction in dy0,
                            search/eval_tech1_600k.py:213-215).
+  * polish_ref          -- (module oracle.polish_ref) numpy restatement of the per-peak polishes of
+                           search/path1_kernel_opt.py.
   * RefLib              -- binding of _ref/libpath1_eval.so, the reference's own evaluator
                            compiled from search/path1_eval_fast.cpp (see Makefile).
 """
@@ -59,6 +61,10 @@ class Oracle:
         L.orc_phase128.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_k2_quad.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+        L.orc_k2_quad_w.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_exact_AB.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_abs_sum.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
         L.orc_abs_sum.restype = C.c_double
         L.orc_gamma_from_G.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
@@ -76,17 +82,37 @@ class Oracle:
         self.L.orc_phase128(P, _p(vi), _p(vf), N, _p(G3), _p(hi), _p(lo))
         return hi, lo
 
-    def k2(self, cands, table, k: float, n_use: int):
-        """(val, dd, dk) in binary128, returned as (P, 3) hi parts and (P, 3) lo parts."""
+    def k2(self, cands, table, k: float, n_use: int, weights=None):
+        """(val, dd, dk) in binary128, returned as (P, 3) hi parts and (P, 3) lo parts.
+
+        weights (length >= n_use) replaces exp(-k gamma^2) per zero when given."""
         vi = np.ascontiguousarray(cands.v_int, dtype=np.uint64)
         vf = np.ascontiguousarray(cands.v_frac, dtype=np.uint64)
         d = np.ascontiguousarray(cands.delta, dtype=np.float64)
         P = vi.shape[0]
         out = np.empty((P, 6), dtype=np.float64)
         G3 = np.ascontiguousarray(table.G3, dtype=np.uint64)
-        self.L.orc_k2_quad(P, _p(vi), _p(vf), _p(d), int(n_use), _p(G3), _p(np.ascontiguousarray(table.c_re)),
-                           _p(np.ascontiguousarray(table.c_im)), float(k), _p(out))
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        if w is not None and w.shape[0] < n_use:
+            raise ValueError("weights shorter than n_use")
+        self.L.orc_k2_quad_w(P, _p(vi), _p(vf), _p(d), int(n_use), _p(G3), _p(np.ascontiguousarray(table.c_re)),
+                             _p(np.ascontiguousarray(table.c_im)), float(k), None if w is None else _p(w), _p(out))
         return out[:, 0::2].copy(), out[:, 1::2].copy()
+
+    def exact_AB(self, cands, table, n_use: int):
+        """A, B (P, n_use) in binary128 rounded to FP64 (compute_exact_mpfr_AB restated)."""
+        vi = np.ascontiguousarray(cands.v_int, dtype=np.uint64)
+        vf = np.ascontiguousarray(cands.v_frac, dtype=np.uint64)
+        d = getattr(cands, "delta", None)
+        d = None if d is None else np.ascontiguousarray(d, dtype=np.float64)
+        P = vi.shape[0]
+        A = np.empty((P, n_use))
+        B = np.empty((P, n_use))
+        G3 = np.ascontiguousarray(table.G3, dtype=np.uint64)
+        self.L.orc_exact_AB(P, _p(vi), _p(vf), None if d is None else _p(d), int(n_use), _p(G3),
+                            _p(np.ascontiguousarray(table.c_re)), _p(np.ascontiguousarray(table.c_im)),
+                            _p(A), _p(B))
+        return A, B
 
     def abs_sum(self, table, k: float, n_use: int) -> float:
         return self.L.orc_abs_sum(int(n_use), _p(np.ascontiguousarray(table.G3)), _p(np.ascontiguousarray(table.c_re)),

@@ -15,6 +15,12 @@ peak2_full_ball.json the interval ball of K2 at the reference's Peak2 point over
                     synthetic zeros below 1.3e6 (table seed 1), k = 1.5e-10, as exact rational
                     endpoints (mpmath iv at 220 bits, summed in 64 worker processes' chunks),
                     plus the binary128 value.
+path1_polish.json   the reference's own polish_single_peak and fast_polish_batch_blas
+                    (search/path1_kernel_opt.py:94-221, the two function bodies executed with
+                    numpy; the module itself needs gmpy2 and its shared library to import) on
+                    A/B of 64 candidates (seed 3) x the first 2,000 zeros of table seed 1 from the
+                    binary128 oracle, with the JP weight and exp(-3e-9 gamma^2); and 16 exact
+                    A/B pairs at 256 bits (mpmath), the compute_exact_mpfr_AB contract (:71-91).
 Each fixture records the SHA-256 of the table arrays so a generator change is detected.
 """
 from __future__ import annotations
@@ -88,6 +94,61 @@ def small_fixture():
     return out
 
 
+REF_PATH1 = "/root/reference/search/path1_kernel_opt.py"
+
+
+def reference_path1_functions():
+    """polish_single_peak and fast_polish_batch_blas from the reference source, executed in a
+    namespace holding only numpy and math."""
+    import ast
+    tree = ast.parse(open(REF_PATH1).read())
+    keep = [n for n in tree.body if isinstance(n, ast.FunctionDef)
+            and n.name in ("polish_single_peak", "fast_polish_batch_blas")]
+    ns = {"np": np, "math": math}
+    exec(compile(ast.Module(body=keep, type_ignores=[]), "path1_kernel_opt.py", "exec"), ns)
+    return ns["polish_single_peak"], ns["fast_polish_batch_blas"]
+
+
+def path1_weights(gamma):
+    u = gamma / gamma[-1]
+    return {"jp": (1.0 - u) * np.cos(np.pi * u) + np.sin(np.pi * u) / np.pi,
+            "g3e-9": np.exp(-3e-9 * gamma * gamma)}
+
+
+def path1_fixture():
+    import mpmath
+    from oracle.oracle import Oracle
+
+    t = synth.make_table(10_000, seed=1)
+    c = synth.make_candidates(64, seed=3)
+    n = 2000
+    A, B = Oracle().exact_AB(c, t, n)
+    single, batch = reference_path1_functions()
+    g = t.gamma[:n]
+    out = {"table": {"n": t.n, "seed": 1, "sha256": table_sha(t)}, "candidates": {"seed": 3, "P": 64},
+           "n_zeros": n, "AB_sha256": hashlib.sha256(A.tobytes() + B.tobytes()).hexdigest(),
+           "source": "search/path1_kernel_opt.py:94-221 executed on oracle A/B"}
+    for name, w in path1_weights(g).items():
+        rows = [single(A[p], B[p], g, w, n_zeros=n, grid_hw=4e-5, grid_steps=40) for p in range(8)]
+        hu, hp, dp = batch(A, B, g, w)
+        out[name] = {"single_first8": [[float(x) for x in r] for r in rows],
+                     "batch": {"h_unpol": [float(x) for x in hu], "h_pol": [float(x) for x in hp],
+                               "ddy_pol": [float(x) for x in dp]}}
+    mpmath.mp.prec = 256
+    pairs = []
+    rng = np.random.default_rng(11)
+    for _ in range(16):
+        p, j = int(rng.integers(64)), int(rng.integers(n))
+        v = mpmath.mpf(int(c.v_int[p])) + mpmath.mpf(int(c.v_frac[p])) / 2 ** 64
+        G = mpmath.mpf(int(t.G3[j, 0])) + mpmath.mpf(int(t.G3[j, 1])) / 2 ** 64 + mpmath.mpf(int(t.G3[j, 2])) / 2 ** 128
+        th = 2 * mpmath.pi * G * v
+        cr, ci = mpmath.mpf(float(t.c_re[j])), mpmath.mpf(float(t.c_im[j]))
+        co, si = mpmath.cos(th), mpmath.sin(th)
+        pairs.append({"p": p, "j": j, "A": float(2 * (cr * co - ci * si)), "B": float(2 * (cr * si + ci * co))})
+    out["exact_AB_pairs_256bit"] = pairs
+    return out
+
+
 _WORKER = {}
 
 
@@ -138,6 +199,9 @@ def main():
     with open(os.path.join(HERE, "small_plain.json"), "w") as f:
         json.dump(small_fixture(), f, indent=1)
     print("wrote small_plain.json", flush=True)
+    with open(os.path.join(HERE, "path1_polish.json"), "w") as f:
+        json.dump(path1_fixture(), f, indent=1)
+    print("wrote path1_polish.json", flush=True)
     if not a.skip_full_ball:
         with open(os.path.join(HERE, "peak2_full_ball.json"), "w") as f:
             json.dump(full_ball_fixture(a.workers), f, indent=1)
