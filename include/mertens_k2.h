@@ -206,6 +206,22 @@ int mb_grid_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *
 int mb_hit_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k, int64_t n_use,
                 uint64_t step_int, uint64_t step_frac, int64_t m0, int64_t n_m, double *out_h);
 
+/* Staged leaf screen of the lattice enumerators: for each leaf v_p (64.64) and m = -3..3,
+ * S_m = sum_j 2|c_j| e^{-k gamma_j^2} cos(2 pi frac((v_p + m step) G_j) + arg c_j) over the first
+ * stage_end[s] zeros; a leaf passes stage s if max_m |S_m| >= threshold[s] and is a hit if it
+ * passes every stage (stage_end increasing, at most 1024 zeros, at most 8 stages).  Hits are
+ * returned in ascending leaf order in out_hits[*n_hits] with their per-stage scores
+ * (out_hit_scores, n_stages per hit); out_scores (nullable, P x n_stages) receives every leaf's
+ * scores, -1 for stages not reached.  More than max_hits hits: MB_ERR_CAPACITY with *n_hits =
+ * the total (the kept subset is then arbitrary).  Replaces ZeroData::fast_screen
+ * (search/fast_mertens_enum.cpp:108-142: 64/128 zeros, thresholds 0.810/0.875) and the GPU leaf
+ * scoring (search/gpu_mertens_stream.cu:192-250: 64/128/256 zeros, 0.78/0.855/0.892), which take
+ * cos from an FP32 table at a 12/14-bit phase; here the 32-bit phase and exact offsets make the
+ * scores accurate to ~1e-6 of sum|a|. */
+int mb_screen(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k, uint64_t step_int,
+              uint64_t step_frac, int n_stages, const int64_t *stage_end, const float *threshold, int64_t max_hits,
+              int64_t *out_hits, float *out_hit_scores, int64_t *n_hits, float *out_scores);
+
 /* ---- per-peak polish contracts of search/path1_kernel_opt.py ------------------------------
  * A_j, B_j = 2 Re, 2 Im of c_j e^{i gamma_j y} and h(ddy) = sum_j w_j (A_j cos(gamma_j ddy) -
  * B_j sin(gamma_j ddy)).  Matrices are row-major (n_peaks, n_zeros) host arrays. */

@@ -26,13 +26,10 @@
 #include "k2_common.cuh"
 #include "k2_fast.h"
 #include "k2_internal.h"
+#include "k2_light.cuh"
 
 namespace mb {
 
-constexpr double MAGIC = 6755399441055744.0;   // 1.5 2^52
-constexpr double TWO_M32 = 2.3283064365386963e-10;
-constexpr double TWO_M64 = 5.421010862427522e-20;
-constexpr double TWO_M96 = 1.2621774483536189e-29;
 
 struct __align__(16) ZLight {   // 64 B
     uint32_t b0, b1, gi, psi32;  // psi32 = round(psi 2^32) + 2 (centres the truncation bias)
@@ -58,26 +55,6 @@ static_assert(FAST_SMEM >= LIGHT_TILE * sizeof(ZLight), "light tile");
 static_assert(FAST_SMEM >= HEAVY_TILE * sizeof(ZHeavy), "heavy tile");
 static_assert(FAST_SMEM >= FAST_THREADS * 4 * 3 * sizeof(double), "reduction buffer");
 
-// Candidate registers shared by both tiers.
-struct CandRegs {
-    uint32_t a0, a1, d1;
-    double A0, A1, D0, D1;      // exact doubles of the limbs a0, a1, d0, d1
-};
-
-MB_DEV CandRegs cand_regs(const CandView &c, int64_t p, bool valid) {
-    Cand64 v{0, 0};
-    if (valid) v = fold_delta(c.vi[p], c.vf[p], c.delta ? c.delta[p] : 0.0);
-    CandRegs r;
-    r.a0 = (uint32_t)v.vi;
-    r.a1 = (uint32_t)(v.vi >> 32);
-    r.d1 = (uint32_t)(v.vf >> 32);
-    r.A0 = u32_to_f64(r.a0);
-    r.A1 = u32_to_f64(r.a1);
-    r.D0 = u32_to_f64((uint32_t)v.vf);
-    r.D1 = u32_to_f64(r.d1);
-    return r;
-}
-
 // Two-sum of floats: s + e = a + b exactly.
 MB_DEV void two_sum(float a, float b, float &s, float &e) {
     s = a + b;
@@ -96,9 +73,7 @@ MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandReg
         const ZLight z = tile[jj];
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
-            uint32_t lo32 = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi;
-            double R = fma(cr[i].A0, z.b0s, fma(cr[i].A1, z.c1s, fma(cr[i].D0, z.gis, fma(cr[i].D1, z.b1s, MAGIC))));
-            int32_t u = (int32_t)(lo32 + (uint32_t)__double2loint(R) + z.psi32);
+            int32_t u = (int32_t)(light_phase32(cr[i], z.b0, z.b1, z.gi, z.b0s, z.c1s, z.gis, z.b1s) + z.psi32);
             float th = (float)u * 1.4629180792671596e-09f;      // 2pi 2^-32
             float s = __sinf(th), co = __cosf(th);
             acc[i][0] = fmaf(z.a, co, acc[i][0]);

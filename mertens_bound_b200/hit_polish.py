@@ -102,3 +102,42 @@ def polish_hits(table: k2.ZeroTable, points: np.ndarray, k: float = 3e-9, thresh
             keep = np.abs(hb) >= thr[s]
             alive = alive[keep]
     return HitResult(best_h, best_dy, stage)
+
+
+# Leaf screens: (zeros at the end of each stage, thresholds) of the reference's proxies.
+SCREEN_GPU = ((64, 128, 256), (0.78, 0.855, 0.892))     # gpu_mertens_stream.cu:203-250
+SCREEN_CPU = ((64, 128), (0.810, 0.875))                # fast_mertens_enum.cpp:108-142
+SCREEN_STEP = 0.0014                                    # offset between the 7 proxy points
+
+
+@dataclass
+class ScreenResult:
+    hits: np.ndarray         # indices of the leaves that passed every stage, ascending
+    hit_scores: np.ndarray   # (n_hits, n_stages) max_m |S_m| after each stage
+    scores: np.ndarray | None  # (P, n_stages) for every leaf (-1 where a stage was not reached)
+
+
+def screen_leaves(table: k2.ZeroTable, points: np.ndarray, k: float = 3e-9, stages=SCREEN_GPU,
+                  step: float = SCREEN_STEP, max_hits: int | None = None, all_scores: bool = False) -> ScreenResult:
+    """The enumerators' staged leaf screen (search/fast_mertens_enum.cpp:108-142,
+    search/gpu_mertens_stream.cu:192-250) on 64.64 points (n, 2): per leaf the sums
+    S_m = sum_j 2|c_j| exp(-k gamma_j^2) cos(gamma_j (y + m step) + arg c_j), m = -3..3, over the
+    zeros of each stage; a leaf survives a stage if max_m |S_m| >= that stage's threshold."""
+    ends, thr = stages
+    ends = np.ascontiguousarray(ends, dtype=np.int64)
+    thr = np.ascontiguousarray(thr, dtype=np.float32)
+    if ends.shape != thr.shape or ends.ndim != 1:
+        raise ValueError("stage ends and thresholds must be 1-D of equal length")
+    pts = np.ascontiguousarray(points, dtype=np.uint64)
+    vi, vf = np.ascontiguousarray(pts[:, 0]), np.ascontiguousarray(pts[:, 1])
+    P, S = vi.shape[0], ends.shape[0]
+    cap = P if max_hits is None else int(max_hits)
+    hits = np.empty(max(cap, 0), dtype=np.int64)
+    hsc = np.empty((max(cap, 0), S), dtype=np.float32)
+    sc = np.empty((P, S), dtype=np.float32) if all_scores else None
+    n = np.zeros(1, dtype=np.int64)
+    st = _fixed(step)
+    check(lib().mb_screen(table.handle, P, ptr(vi), ptr(vf), float(k), st >> 64, st & MASK64, S, ptr(ends),
+                          ptr(thr), cap, ptr(hits), ptr(hsc), ptr(n), ptr(sc)))
+    m = int(n[0])
+    return ScreenResult(hits[:m].copy(), hsc[:m].copy(), sc)
