@@ -42,13 +42,13 @@ UNIT = "zero-terms/s"
 T0, K_GAUSS, P_PER_GPU, TOL = 3e5, 3e-9, 4096, 1e-10
 WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 candidates v~3.5e18 "
             "per GPU, k=3e-9, K2 + dK2/ddelta + dK2/dk per candidate, a-priori |err| <= 1e-10")
-# Thread instructions per zero-term of the light-tier kernel (the dominant kernel) for each
-# candidates-per-thread setting, from the ncu captures summarised in
-# profiles/k2_light_kernel_search_scoring.md.
-LIGHT_INST_PER_TERM = {2: 24.6, 3: 25.1, 4: 21.2}
+# Warp instructions per warp of zero-terms (= thread instructions per zero-term) of the light-tier
+# kernel (the dominant kernel) for each candidates-per-thread setting, from the ncu capture of
+# `bench.py --profile-case search` summarised in profiles/k2_light_kernel_search_scoring.md.
+LIGHT_INST_PER_TERM = {2: 23.43, 3: 25.67, 4: 20.07}
 # DRAM bytes per light launch on this workload (same captures): reads of the zero tiles and
 # candidates; writes ~0.
-LIGHT_DRAM_BYTES = {2: 16517632, 3: 16416512, 4: 16380672}
+LIGHT_DRAM_BYTES = {2: 16419840, 3: 16779520, 4: 16581120}
 REF_SAMPLE_CANDS = 64
 
 
@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="skip the summary of the other workloads")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--profile-case", choices=["small", "search"], default=None,
+                    help="run a fixed case for ncu captures (no timing): 'small' = zeros below 1e5 x "
+                         "2,048 candidates, all kernels of one plan run; 'search' = the bench workload, "
+                         "each kernel launched alone once (plain; light tier at 2, 3, 4 candidates per "
+                         "thread; heavy tier)")
     return ap.parse_args()
 
 
@@ -297,14 +302,47 @@ def run_ours(args):
     plan.close()
     table.close()
     if world == 1 and not args.no_workloads:
-        line["workloads"] = other_workloads(torch, dev, timed)
+        line["workloads"] = other_workloads(torch, dev, timed, cpu_baseline=not args.no_cpu_baseline)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def other_workloads(torch, dev, timed):
+def _ball_chunk(args):
+    """One worker's share of the interval restatement (oracle/interval.py) of the certified sum."""
+    from oracle.interval import k2_ball
+    vi, vf, G3, cre, cim, k = args
+    k2_ball(vi, vf, 0.0, G3, cre, cim, k, len(cre))
+    return len(cre)
+
+
+def certified_cpu_rate(big, pk, n_full: int, per_worker: int = 1500):
+    """Zeros/s of the certified sum on the host cores: the 220-bit interval restatement of
+    certify_K2.work (python-flint, the reference's ball library, is not installed), one chunk of
+    per_worker zeros per core spread over the table, in a spawn pool (the GPU is already in use)."""
+    import multiprocessing as mp
+    n = os.cpu_count() or 1
+    starts = np.linspace(0, big.n - per_worker, n).astype(int)
+    tasks = [(int(pk.v_int[0]), int(pk.v_frac[0]), big.G3[a:a + per_worker].copy(), big.c_re[a:a + per_worker].copy(),
+              big.c_im[a:a + per_worker].copy(), 1.5e-10) for a in starts]
+    try:
+        with mp.get_context("spawn").Pool(n) as pool:
+            warm = [(a, b, G[:16], c, d, k) for a, b, G, c, d, k in tasks]
+            pool.map_async(_ball_chunk, [(a, b, G, c[:16], d[:16], k) for a, b, G, c, d, k in warm],
+                           chunksize=1).get(timeout=300)         # imports
+            t0 = time.perf_counter()
+            done = sum(pool.map_async(_ball_chunk, tasks, chunksize=1).get(timeout=600))
+            secs = time.perf_counter() - t0
+    except Exception as e:                                       # a worker failed or timed out
+        return {"kind": "port", "unavailable": f"{type(e).__name__}: {e}"}
+    rate = done / secs
+    return {"kind": "port", "cores": n, "zeros_per_s": rate, "full_sum_s_extrapolated": n_full / rate,
+            "sample": f"{done} zeros ({n} chunks of {per_worker} spread over the table), mpmath iv at 220 bits "
+                      "restating certify_K2.work; python-flint is not installed"}
+
+
+def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
     """The other four workload shapes, measured briefly on the same GPU (summary numbers)."""
     from mertens_bound_b200 import k2, synth, _lib
     from mertens_bound_b200._lib import check
@@ -357,6 +395,8 @@ def other_workloads(torch, dev, timed):
         out["certified_full"] = {"zeros": tb.count_below(1.3e6), "seconds": statistics.median(ts),
                                  "lo": float(lo[0]), "hi": float(hi[0]), "width": float(hi[0] - lo[0]),
                                  "abs_sum_hi": float(ab[0])}
+        if cpu_baseline:
+            out["certified_full"]["cpu_baseline"] = certified_cpu_rate(big, pk, out["certified_full"]["zeros"])
 
         # batched_uneven: 16,384 candidates in 12 groups over T x k
         counts, ks, Ts = synth.batched_uneven_groups()
@@ -447,9 +487,62 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args):
+    """Fixed cases for ncu captures (no timing, no bench line).
+      small   zeros below 1e5, 2,048 candidates: the chosen form (light tier at 4 candidates per
+              thread) args.warmup + args.steps times, then the plain kernel once (~40 MB on the
+              device);
+      search  the bench workload (zeros below 3e5, 4,096 candidates): the plain kernel once, the
+              light tier alone at 2, 3 and 4 candidates per thread, the heavy tier alone (~80 MB)."""
+    import torch
+    from mertens_bound_b200 import k2, synth, _lib
+    from mertens_bound_b200._lib import check
+
+    dev = torch.device("cuda", 0)
+    T, P = (1e5, 2048) if args.profile_case == "small" else (T0, P_PER_GPU)
+    data = synth.make_table_below(T, seed=1)
+    cands = synth.make_candidates(P, seed=3)
+    table = k2.ZeroTable.from_data(data)
+    vi = torch.from_numpy(cands.v_int.view(np.int64)).to(dev)
+    vf = torch.from_numpy(cands.v_frac.view(np.int64)).to(dev)
+    dl = torch.zeros(P, dtype=torch.float64, device=dev)
+    out = torch.empty(3, P, dtype=torch.float64, device=dev)
+    sptr = torch.cuda.current_stream(dev).cuda_stream
+    L = _lib.lib()
+    plan = k2.Plan(table, [P], [K_GAUSS], [T], tol=TOL)
+
+    def tiers(n):
+        check(L.mb_plan_run_tiers_dev(plan.handle, n, vi.data_ptr(), vf.data_ptr(), dl.data_ptr(),
+                                      out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), sptr))
+
+    def plain():
+        check(L.mb_k2_plain_dev(table.handle, P, vi.data_ptr(), vf.data_ptr(), dl.data_ptr(), K_GAUSS, T,
+                                out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), sptr))
+
+    if args.profile_case == "small":
+        plan.configure(4, 0, 1.0)
+        for _ in range(args.warmup + args.steps):
+            tiers(3)
+        plain()
+    else:
+        plain()
+        for cpt in (2, 3, 4):
+            plan.configure(cpt, 0, 1.0)
+            tiers(2)
+        tiers(1)
+    torch.cuda.synchronize(dev)
+    ht, lt = C_double_pair(L.mb_plan_tier_terms, plan.handle)
+    print(json.dumps({"profile_case": args.profile_case, "zeros": table.count_below(T), "candidates": P,
+                      "heavy_terms": ht, "light_terms": lt}), flush=True)
+    plan.close()
+    table.close()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

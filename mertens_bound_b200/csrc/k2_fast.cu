@@ -4,20 +4,20 @@
 // from an a-priori error bound (host, k2_plan.cu):
 //   heavy tier  j <  n_h : 64-bit phase (3 IMAD.lo + 8 DFMA, error ~2^-48 turn), quarter-turn
 //                          FP64 polynomials, FP64 accumulation.          -> k2_heavy_kernel
-//   light tier  j >= n_h : 32-bit phase (3 IMAD.lo + 4 DFMA), MUFU sin/cos of the reduced
-//                          phase, FP32 accumulation flushed every LIGHT_FLUSH terms by two-sum
-//                          into float-float partials.                    -> k2_light_kernel
-// The heavy kernel is persistent with one CTA per SM (FP64-pipe bound); the light kernel is
-// launched concurrently on a second stream with one CTA per work item and fills the rest of
-// each SM (XU / FMA / integer pipes), so the two tiers overlap on every SM.
+//   light tier  j >= n_h : 32-bit phase (3 IMAD.lo + 4 DFMA in two chains), MUFU sin/cos of
+//                          the reduced phase, FP32 accumulation flushed every LIGHT_FLUSH terms
+//                          into FP64 partials.                           -> k2_light_kernel
+// The heavy kernel is persistent with two CTAs per SM (FP64-pipe bound); the light kernel is
+// launched concurrently on a second stream with one CTA per work item and takes each SM as the
+// heavy CTAs retire (XU / FMA / integer pipes), so the tiers overlap.
 //
 // Phase algebra (v = a1 2^32 + a0 + (d1 2^-32 + d0 2^-64), G = gI + b1 2^-32 + b0 2^-64 +
 // c1 2^-96 + c0 2^-128, all limbs 32-bit):
 //   frac(vG) 2^32 = [a1 b0 + a0 b1 + d1 gI]                       (exact mod 2^32, IMAD.lo)
 //                 + (a0 b0 + a1 c1 + d0 gI + d1 b1) 2^-32           (< 2^34, FP64)
 //                 + (a1 c0 + a0 c1 + d1 b0 + d0 b1) 2^-64 + ...     (< 4 units)
-// The FP64 sum is formed on top of 1.5 2^52, so each DFMA rounds it to an integer and the low
-// mantissa word holds it mod 2^32 (error <= 2 units of 2^-32 turn).
+// The FP64 sums are formed on top of 1.5 2^52, so each DFMA rounds to an integer and the low
+// mantissa words hold them mod 2^32 (error <= 2 units of 2^-32 turn; k2_light.cuh).
 // arg(c)/2pi (psi) is added to the phase, so each term is a cos(2pi u) with a = 2|c| w.
 #include <algorithm>
 #include <cmath>
@@ -55,16 +55,9 @@ static_assert(FAST_SMEM >= LIGHT_TILE * sizeof(ZLight), "light tile");
 static_assert(FAST_SMEM >= HEAVY_TILE * sizeof(ZHeavy), "heavy tile");
 static_assert(FAST_SMEM >= FAST_THREADS * 4 * 3 * sizeof(double), "reduction buffer");
 
-// Two-sum of floats: s + e = a + b exactly.
-MB_DEV void two_sum(float a, float b, float &s, float &e) {
-    s = a + b;
-    float bb = s - a;
-    e = (a - (s - bb)) + (b - bb);
-}
-
 template <int CPT>
 MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
-                       float (&hi)[CPT][3], float (&lo)[CPT][3]) {
+                       double (&sum)[CPT][3]) {
     float acc[CPT][3];
 #pragma unroll
     for (int i = 0; i < CPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
@@ -73,7 +66,7 @@ MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandReg
         const ZLight z = tile[jj];
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
-            int32_t u = (int32_t)(light_phase32(cr[i], z.b0, z.b1, z.gi, z.b0s, z.c1s, z.gis, z.b1s) + z.psi32);
+            int32_t u = (int32_t)light_phase32(cr[i], z.b0, z.b1, z.gi, z.b0s, z.c1s, z.gis, z.b1s, z.psi32);
             float th = (float)u * 1.4629180792671596e-09f;      // 2pi 2^-32
             float s = __sinf(th), co = __cosf(th);
             acc[i][0] = fmaf(z.a, co, acc[i][0]);
@@ -86,10 +79,7 @@ MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandReg
             for (int i = 0; i < CPT; ++i)
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
-                    float s, e;
-                    two_sum(hi[i][q], acc[i][q], s, e);
-                    hi[i][q] = s;
-                    lo[i][q] += e;
+                    sum[i][q] += (double)acc[i][q];
                     acc[i][q] = 0.f;
                 }
         }
@@ -97,12 +87,7 @@ MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandReg
 #pragma unroll
     for (int i = 0; i < CPT; ++i)
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            float s, e;
-            two_sum(hi[i][q], acc[i][q], s, e);
-            hi[i][q] = s;
-            lo[i][q] += e;
-        }
+        for (int q = 0; q < 3; ++q) sum[i][q] += (double)acc[i][q];
 }
 
 template <int CPT>
@@ -208,23 +193,18 @@ MB_DEV void light_item(const FastItem &it, const FastGroup &gr, const TabView &t
 #pragma unroll
     for (int i = 0; i < CPT; ++i) cr[i] = cand_regs(c, cbase + i, cbase + i < cend);
     ZLight *tile = reinterpret_cast<ZLight *>(smem);
-    float hi[CPT][3], lo[CPT][3];
+    double res[CPT][3];
 #pragma unroll
     for (int i = 0; i < CPT; ++i)
 #pragma unroll
-        for (int q = 0; q < 3; ++q) hi[i][q] = lo[i][q] = 0.f;
+        for (int q = 0; q < 3; ++q) res[i][q] = 0.0;
     for (int64_t tb = it.z0; tb < it.z1; tb += LIGHT_TILE) {
         __syncthreads();
         int64_t j = tb + threadIdx.x;
         if (threadIdx.x < LIGHT_TILE && j < it.z1) stage_light(t, j, gr.k, gr.w, tile[threadIdx.x]);
         __syncthreads();
-        light_tile<CPT>(tile, (int)min((int64_t)LIGHT_TILE, it.z1 - tb), zw, nzw, cr, hi, lo);
+        light_tile<CPT>(tile, (int)min((int64_t)LIGHT_TILE, it.z1 - tb), zw, nzw, cr, res);
     }
-    double res[CPT][3];
-#pragma unroll
-    for (int i = 0; i < CPT; ++i)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) res[i][q] = (double)hi[i][q] + (double)lo[i][q];
     finish_item<CPT>(it, gr, res, warp, lane, zw, cbase, cend, partial, smem);
 }
 
@@ -254,7 +234,7 @@ MB_DEV void heavy_item(const FastItem &it, const FastGroup &gr, const TabView &t
 }
 
 // Heavy tier: persistent, items pulled from an atomic counter (largest first).  At most 128
-// registers, so one heavy CTA leaves half of the SM's registers to light CTAs beside it.
+// registers per thread: two CTAs per SM.
 __global__ void __launch_bounds__(FAST_THREADS, 2)
 k2_heavy_kernel(TabView t, CandView c, const FastItem *items, int n_items, const FastGroup *groups,
                 int *counter, double *partial) {
@@ -401,7 +381,10 @@ int calibrate_issue(int device, double *thread_inst_per_s) {
 int heavy_grid_size(int device, unsigned *grid) {
     int sms = 148;
     MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    *grid = (unsigned)sms;   // one CTA per SM leaves room for light CTAs beside it
+    // two CTAs per SM (16 warps): the heavy tier is FP64-latency bound with fewer; light CTAs
+    // take each SM's registers as the heavy CTAs retire (measured faster than one CTA per SM
+    // beside a light CTA)
+    *grid = (unsigned)(2 * sms);
     return MB_OK;
 }
 

@@ -43,13 +43,16 @@ MB_DEV CandRegs cand_regs(const CandView &c, int64_t p, bool valid) {
     return cand_regs_of(v);
 }
 
-// frac(vG) 2^32 mod 2^32 to within a few units; the zero's limbs b0, b1, gI and its scaled
-// doubles b0s = b0 2^-32, c1s = c1 2^-32, gis = gI 2^-32, b1s = b1 2^-32.
+// add + frac(vG) 2^32 mod 2^32 to within a few units; the zero's limbs b0, b1, gI and its
+// scaled doubles b0s = b0 2^-32, c1s = c1 2^-32, gis = gI 2^-32, b1s = b1 2^-32.  The four
+// middle products form two independent DFMA chains (each rounded to an integer on top of
+// 1.5 2^52; four roundings of <= 1/2 unit in all), so the dependent latency is two DFMAs.
 MB_DEV uint32_t light_phase32(const CandRegs &c, uint32_t b0, uint32_t b1, uint32_t gi, double b0s, double c1s,
-                              double gis, double b1s) {
-    const uint32_t lo32 = c.a1 * b0 + c.a0 * b1 + c.d1 * gi;
-    const double R = fma(c.A0, b0s, fma(c.A1, c1s, fma(c.D0, gis, fma(c.D1, b1s, MAGIC))));
-    return lo32 + (uint32_t)__double2loint(R);
+                              double gis, double b1s, uint32_t add) {
+    const uint32_t lo32 = c.a1 * b0 + c.a0 * b1 + c.d1 * gi + add;
+    const double R1 = fma(c.A0, b0s, fma(c.A1, c1s, MAGIC));
+    const double R2 = fma(c.D0, gis, fma(c.D1, b1s, MAGIC));
+    return lo32 + (uint32_t)__double2loint(R1) + (uint32_t)__double2loint(R2);
 }
 
 }  // namespace mb

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(SCREEN_THREADS) screen_kernel(const ZScreen *z
         const int end = sa.stage_end[s];
         for (; j < end; ++j) {
             const ZScreen z = tile[j];
-            const int32_t u = (int32_t)(light_phase32(cr, z.b0, z.b1, z.gi, z.b0s, z.c1s, z.gis, z.b1s) + z.psi32);
+            const int32_t u = (int32_t)light_phase32(cr, z.b0, z.b1, z.gi, z.b0s, z.c1s, z.gis, z.b1s, z.psi32);
             const float th = (float)u * 1.4629180792671596e-09f;   // 2pi 2^-32
             const float sn = __sinf(th), cs = __cosf(th);
             S[3] = fmaf(z.a, cs, S[3]);
