@@ -142,6 +142,15 @@ int mb_table_add_weights(mb_table *t, const double *w, int64_t n, int *slot);
 int mb_plan_create_weighted(mb_table *t, int n_groups, const int64_t *counts, const double *ks, const double *Ts,
                             const int *weight_slots, double tol, mb_plan **out);
 int mb_plan_destroy(mb_plan *p);
+/* Tail skip: give the share skip_frac (0 .. 0.25) of tol to not evaluating, per group, the zeros
+ * beyond the point where the remaining sum of 2|c| w is <= skip_frac * tol (the Gaussian makes
+ * most zeros below a large T negligible at tol = 1e-10: ~76% of them at T = 3e5, k = 3e-9).
+ * The light tier keeps (1/2 - skip_frac) tol; the group bound includes the skipped sum; the
+ * derivative outputs omit the same zeros.  0 (the default) evaluates every zero below T, as the
+ * reference does.  No reference counterpart (it sums every zero below its cutoff). */
+int mb_plan_set_skip(mb_plan *p, double skip_frac);
+/* Zeros evaluated for group g (count_below(T) without a tail skip). */
+int mb_plan_group_zeros(const mb_plan *p, int g, int64_t *n_eval);
 /* Override the tile shape of group g: cpt in {1,2,4} candidates per thread, nzw in {1,2,4,8}
  * warps splitting the zeros, chunk sizes in zeros (0 = automatic; multiples of 128 / 256). */
 int mb_plan_set_shape(mb_plan *p, int g, int cpt, int nzw, int64_t heavy_chunk, int64_t light_chunk);

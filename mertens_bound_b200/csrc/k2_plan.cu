@@ -21,7 +21,8 @@ struct mb_plan {
     std::vector<int> wslot;        // per group: table weight vector, or -1 for exp(-k gamma^2)
     std::vector<FastGroup> groups;
     std::vector<FastItem> items;
-    std::vector<int64_t> n_T, n_heavy;
+    std::vector<int64_t> n_T, n_eval, n_heavy;   // zeros below T, zeros evaluated, heavy zeros
+    double skip_frac = 0.0;        // share of tol given to skipping the tail of each group
     std::vector<double> err_bound, sum_abs;
     std::vector<int> shape_nzw;
     std::vector<int64_t> heavy_chunk, light_chunk;
@@ -73,10 +74,14 @@ int default_nzw(int64_t P, int cpt) {
     return nzw;
 }
 
-// Tier boundary: the smallest n_h with EPS_LIGHT * sum_{j>=n_h} a_j <= budget, where
-// a_j = 2|c_j| exp(-k gamma_j^2) bounds |term_j|.  Returns the bound of the whole sum.
-void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, double tol, int64_t &n_h, double &bound,
-                double &sabs) {
+// Tier boundary and tail skip, with a_j = 2|c_j| w_j >= |term_j| (w_j = exp(-k gamma_j^2) or the
+// group's weight vector):
+//   n_eval: the smallest n with sum_{n <= j < n_use} a_j <= skip_frac * tol -- those zeros are
+//           not evaluated (skip_frac = 0: every zero below T is evaluated);
+//   n_h:    the smallest n_h with EPS_LIGHT * sum_{n_h <= j < n_eval} a_j <= (1/2 - skip_frac) tol.
+// Returns the a-priori bound of |K2 error| (skipped sum + tier errors + FP64 roundings).
+void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, double tol, double skip_frac,
+                int64_t &n_eval, int64_t &n_h, double &bound, double &sabs) {
     std::vector<double> a(n_use);
     double total = 0;
     for (int64_t j = 0; j < n_use; ++j) {
@@ -84,19 +89,37 @@ void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, doub
         a[j] = 2.0 * t.h_alpha[j] * (wts ? std::fabs(wts[j]) : std::exp(-k * g * g));
         total += a[j];
     }
-    const double budget = 0.5 * tol;
+    double skipped = 0;
+    n_eval = n_use;
+    if (skip_frac > 0)
+        for (int64_t j = n_use - 1; j >= 0; --j) {
+            if (skipped + a[j] > skip_frac * tol) break;
+            skipped += a[j];
+            n_eval = j;
+        }
+    const double budget = (0.5 - skip_frac) * tol;
     double tail = 0;
-    n_h = n_use;
-    for (int64_t j = n_use - 1; j >= 0; --j) {
+    n_h = n_eval;
+    for (int64_t j = n_eval - 1; j >= 0; --j) {
         if ((tail + a[j]) * EPS_LIGHT > budget) break;
         tail += a[j];
         n_h = j;
     }
-    double heavy = total - tail;
+    const double evaluated = total - skipped;
+    double heavy = evaluated - tail;
     // FP64 accumulation and reduction of the heavy sum and of the light partials: at most
     // ~(terms per thread + chunks) roundings of 2^-53 relative; 1e-13 relative is a safe cover.
-    bound = EPS_LIGHT * tail + EPS_HEAVY * heavy + 1e-13 * total;
+    bound = skipped + EPS_LIGHT * tail + EPS_HEAVY * heavy + 1e-13 * evaluated;
     sabs = total;
+}
+
+void replan_tiers(mb_plan *p) {
+    const Table &t = *p->table;
+    for (int g = 0; g < p->n_groups; ++g) {
+        const double *wh = p->wslot[g] >= 0 ? t.h_weights[p->wslot[g]].data() : nullptr;
+        plan_tiers(t, p->n_T[g], p->ks[g], wh, p->tol, p->skip_frac, p->n_eval[g], p->n_heavy[g],
+                   p->err_bound[g], p->sum_abs[g]);
+    }
 }
 
 // Work items.  Heavy items (FP64 tier) use HEAVY_CPT candidates per thread and are pulled by
@@ -110,7 +133,7 @@ int build_items(mb_plan *p, int sms) {
     auto hb = [&](int g) { return std::max<int64_t>(0, p->z_begin); };
     auto he = [&](int g) { return std::min(p->n_heavy[g], p->z_end); };
     auto lb = [&](int g) { return std::max(p->n_heavy[g], p->z_begin); };
-    auto le = [&](int g) { return std::min(p->n_T[g], p->z_end); };
+    auto le = [&](int g) { return std::min(p->n_eval[g], p->z_end); };
     double Wh = 0, Wl = 0;
     for (int g = 0; g < p->n_groups; ++g) {
         Wh += (double)p->counts[g] * std::max<int64_t>(0, he(g) - hb(g));
@@ -271,6 +294,7 @@ extern "C" int mb_plan_create_weighted(mb_table *h, int n_groups, const int64_t 
     p->ks.assign(ks, ks + n_groups);
     p->Ts.assign(Ts, Ts + n_groups);
     p->n_T.resize(n_groups);
+    p->n_eval.resize(n_groups);
     p->n_heavy.resize(n_groups);
     p->err_bound.resize(n_groups);
     p->sum_abs.resize(n_groups);
@@ -281,10 +305,9 @@ extern "C" int mb_plan_create_weighted(mb_table *h, int n_groups, const int64_t 
     if (weight_slots) p->wslot.assign(weight_slots, weight_slots + n_groups);
     for (int g = 0; g < n_groups; ++g) {
         p->n_T[g] = t.count_below(Ts[g]);
-        const double *wh = p->wslot[g] >= 0 ? t.h_weights[p->wslot[g]].data() : nullptr;
-        plan_tiers(t, p->n_T[g], ks[g], wh, tol, p->n_heavy[g], p->err_bound[g], p->sum_abs[g]);
         p->shape_nzw[g] = default_nzw(counts[g], p->light_cpt);
     }
+    replan_tiers(p);
     int st = upload(p);
     if (st != MB_OK) {
         free_dev(p);
@@ -343,6 +366,26 @@ extern "C" int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, doubl
     }
     MB_TRY(device_guard(p->table->device));
     return upload(p);
+}
+
+// Give the share skip_frac (0 .. 1/4) of tol to not evaluating each group's negligible tail: the
+// zeros beyond the point where the remaining sum of 2|c| w is <= skip_frac tol are skipped, and
+// the light tier keeps (1/2 - skip_frac) tol.  The bound of mb_plan_group_info includes the
+// skipped sum.  (The derivative outputs then omit sum 2|c| w gamma and 2|c| w gamma^2 over the
+// same zeros.)  0 restores the evaluation of every zero below T.
+extern "C" int mb_plan_set_skip(mb_plan *p, double skip_frac) {
+    MB_CHECK_ARG(p, "mb_plan_set_skip: null plan");
+    MB_CHECK_ARG(skip_frac >= 0.0 && skip_frac <= 0.25, "mb_plan_set_skip: skip_frac=%g (0 .. 0.25)", skip_frac);
+    p->skip_frac = skip_frac;
+    replan_tiers(p);
+    MB_TRY(device_guard(p->table->device));
+    return upload(p);
+}
+
+extern "C" int mb_plan_group_zeros(const mb_plan *p, int g, int64_t *n_eval) {
+    MB_CHECK_ARG(p && n_eval && g >= 0 && g < p->n_groups, "mb_plan_group_zeros: bad plan/group");
+    *n_eval = p->n_eval[g];
+    return MB_OK;
 }
 
 // Restrict every group to the zeros [j0, j1) (intersected with its [0, n_T)): a zero-range shard.
@@ -441,7 +484,7 @@ extern "C" int mb_plan_tier_terms(const mb_plan *p, double *heavy_terms, double 
     double h = 0, l = 0;
     for (int g = 0; g < p->n_groups; ++g) {
         h += (double)p->counts[g] * p->n_heavy[g];
-        l += (double)p->counts[g] * (p->n_T[g] - p->n_heavy[g]);
+        l += (double)p->counts[g] * (p->n_eval[g] - p->n_heavy[g]);
     }
     if (heavy_terms) *heavy_terms = h;
     if (light_terms) *light_terms = l;

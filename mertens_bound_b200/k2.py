@@ -158,6 +158,10 @@ class Plan:
     def set_shape(self, g: int, cpt: int, nzw: int, heavy_chunk: int = 0, light_chunk: int = 0):
         check(_lib.lib().mb_plan_set_shape(self.handle, g, cpt, nzw, heavy_chunk, light_chunk))
 
+    def set_skip(self, skip_frac: float):
+        """Skip each group's negligible tail of zeros, giving it skip_frac (<= 0.25) of tol."""
+        check(_lib.lib().mb_plan_set_skip(self.handle, float(skip_frac)))
+
     def configure(self, light_cpt: int, nzw_shift: int, chunk_scale: float):
         check(_lib.lib().mb_plan_configure(self.handle, int(light_cpt), int(nzw_shift), float(chunk_scale)))
         self.config = (int(light_cpt), int(nzw_shift), float(chunk_scale))
@@ -180,8 +184,11 @@ class Plan:
 
     def group_info(self, g: int):
         nT, nh, eb, sa = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
+        ne = C.c_int64()
         check(_lib.lib().mb_plan_group_info(self.handle, g, C.byref(nT), C.byref(nh), C.byref(eb), C.byref(sa)))
-        return {"n_T": nT.value, "n_heavy": nh.value, "err_bound": eb.value, "sum_abs": sa.value}
+        check(_lib.lib().mb_plan_group_zeros(self.handle, g, C.byref(ne)))
+        return {"n_T": nT.value, "n_eval": ne.value, "n_heavy": nh.value, "err_bound": eb.value,
+                "sum_abs": sa.value}
 
     def run(self, cands):
         """Host arrays in, host arrays out (graph replay through pinned staging)."""

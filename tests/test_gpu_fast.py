@@ -100,3 +100,24 @@ def test_all_heavy_when_tolerance_tight(table, small_table, oracle):
         val, _, _ = plan.run(cd)
     ohi, _ = oracle.k2(cd, small_table, 3e-9, small_table.n)
     assert np.max(np.abs(val - ohi[:, 0])) < 1e-12
+
+
+def test_tail_skip_within_bound(gpu, oracle):
+    """Skipping the negligible tail keeps |K2 - oracle| within the plan's bound (which now
+    includes the skipped sum) and evaluates fewer zeros."""
+    data = synth.make_table(60_000, seed=6)
+    cd = synth.make_candidates(96, seed=61)
+    k = 1e-8      # the Gaussian makes the zeros above gamma ~ 3e4 negligible at 1e-10
+    ohi, _ = oracle.k2(cd, data, k, data.n)
+    with k2.ZeroTable.from_data(data) as t, k2.Plan(t, [96], [k], [math.inf], tol=TOL) as plan:
+        full, _, _ = plan.run(cd)
+        plan.set_skip(0.25)
+        gi = plan.group_info(0)
+        assert gi["n_eval"] < gi["n_T"] == data.n
+        assert gi["err_bound"] <= TOL
+        val, _, _ = plan.run(cd)
+        assert np.max(np.abs(val - ohi[:, 0])) <= gi["err_bound"]
+        plan.set_skip(0.0)
+        assert plan.group_info(0)["n_eval"] == data.n
+        again, _, _ = plan.run(cd)
+        assert np.array_equal(again, full)
