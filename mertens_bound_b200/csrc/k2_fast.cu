@@ -98,10 +98,11 @@ MB_DEV void heavy_tile(const ZHeavy *tile, int nt, int zl, int ZL, const CandReg
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
             uint32_t lo32 = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi;
+            // the chain starts from psi = arg(c)/2pi, so the last product's DFMA also adds it
             double F = fma(cr[i].A0, z.b0s, fma(cr[i].A1, z.c1s, fma(cr[i].D0, z.gis,
                        fma(cr[i].D1, z.b1s, fma(cr[i].A1, z.c0t, fma(cr[i].A0, z.c1t,
-                       fma(cr[i].D1, z.b0t, cr[i].D0 * z.b1t)))))));
-            double y = fma(u32_to_f64(lo32), TWO_M32, F) + z.psi;
+                       fma(cr[i].D1, z.b0t, fma(cr[i].D0, z.b1t, z.psi))))))));
+            double y = fma(u32_to_f64(lo32), TWO_M32, F);
             double sn, cs;
             sincos_turns_quad(y, sn, cs);
             acc[i][0] = fma(z.a, cs, acc[i][0]);
