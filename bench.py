@@ -156,6 +156,18 @@ def reference_rate(table, cands, k: float, n_use: int, seconds: float, steps: in
 
 # ---------------------------------------------------------------- our arm
 
+def hbm_line(bytes_per_launch: float, ms: float) -> dict:
+    """The light kernel's DRAM traffic as a fraction of the measured HBM copy peak (it is not the
+    binding roof: the kernel is issue bound)."""
+    gbs = bytes_per_launch / (ms * 1e-3) / 1e9
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, src = float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        peak, src = 6650.0, "fallback"
+    return {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak, "peak_source": src}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -247,6 +259,14 @@ def run_ours(args):
     value = world * terms * args.steps / (total_ms * 1e-3)
     ms_per_step = total_ms / args.steps
     diff = (out - ref).abs().max(dim=1).values.cpu().numpy()
+    # error against rigorous enclosures: the certified interval kernel on a 64-candidate subsample
+    # (the error of a value inside nothing wider than the interval is below |val - mid| + width/2)
+    sub = cands.subset(np.arange(64))
+    clo, chi, _ = k2.k2_certified(table, sub, K_GAUSS, T0)
+    got = out[0, :64].cpu().numpy()
+    mid, half = 0.5 * (clo + chi), 0.5 * (chi - clo)
+    err_vs_cert = {"candidates": 64, "max_abs_err": float(np.max(np.abs(got - mid) + half)),
+                   "max_interval_width": float(np.max(chi - clo)), "a_priori_bound": gi["err_bound"]}
 
     # per-tier kernels on their own (roofline of the dominant kernel)
     light_ms = statistics.median(timed(lambda: fast(2), 5, 1))
@@ -293,6 +313,7 @@ def run_ours(args):
         "plain_fp64": {"value": world * plain_rate, "ms_per_step": statistics.median(plain_ms)},
         "speedup_vs_plain": world * plain_rate and value / (world * plain_rate),
         "max_abs_diff_vs_plain": {"val": float(diff[0]), "dd": float(diff[1]), "dk": float(diff[2])},
+        "err_vs_certified": err_vs_cert,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * P, "d2h_bytes_per_step": 3 * 8 * P},
         "roofline": {"bound": "issue", "kernel": "k2_light_kernel", "achieved": light_achieved / 1e12,
                      "peak": peak / 1e12, "unit": "T thread-inst/s", "frac": light_achieved / peak,
@@ -300,7 +321,8 @@ def run_ours(args):
                      "per_term_inst": inst_per_term, "light_ms": light_ms,
                      "heavy_ms": heavy_ms, "light_terms": lt, "heavy_terms": ht,
                      "peak_source": "measured live: FFMA issue rate (mb_calibrate_issue); MEASURED_PEAKS.json "
-                                    "has only HBM and bf16-tensor peaks, neither binds this kernel"},
+                                    "has only HBM and bf16-tensor peaks, neither binds this kernel",
+                     "hbm": hbm_line(LIGHT_DRAM_BYTES[tuned["config"][0]], light_ms)},
         "clocks": clocks,
         "gpu_launches": 3 * args.steps,
         "tail_skip": tail_skip,
