@@ -312,18 +312,23 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
     const TabView tv = view(t);
     const bool heavy = (tiers & 1) && pd.n_heavy > 0;
     const bool light = (tiers & 2) && pd.n_light > 0;
+    // with both tiers: fork the heavy tier onto the table's side stream, concurrently with the
+    // light tier on s; with one tier everything stays on s
+    const bool fork = heavy && light;
+    cudaStream_t hs = fork ? t.side : s;
     if (heavy) {
-        // fork: heavy tier on the table's side stream, concurrently with the light tier on s
-        MB_CUDA(cudaEventRecord(t.ev_fork, s));
-        MB_CUDA(cudaStreamWaitEvent(t.side, t.ev_fork, 0));
-        MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), t.side));
-        k2_heavy_kernel<<<pd.heavy_grid, FAST_THREADS, 0, t.side>>>(tv, c, pd.items, pd.n_heavy, pd.groups,
-                                                                    pd.counter, pd.partial);
+        if (fork) {
+            MB_CUDA(cudaEventRecord(t.ev_fork, s));
+            MB_CUDA(cudaStreamWaitEvent(t.side, t.ev_fork, 0));
+        }
+        MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), hs));
+        k2_heavy_kernel<<<pd.heavy_grid, FAST_THREADS, 0, hs>>>(tv, c, pd.items, pd.n_heavy, pd.groups,
+                                                                pd.counter, pd.partial);
         MB_CUDA(cudaGetLastError());
-        MB_CUDA(cudaEventRecord(t.ev_join, t.side));
+        if (fork) MB_CUDA(cudaEventRecord(t.ev_join, t.side));
     }
     if (light) MB_TRY(launch_light(tv, pd, c, s));
-    if (heavy) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
+    if (fork) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
     fast_reduce_kernel<<<(unsigned)((c.P * 32 + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
                                                                      d_val, d_dd, d_dk);
     MB_CUDA(cudaGetLastError());
