@@ -266,6 +266,14 @@ int mb_fast_polish_batch(int64_t n_peaks, int64_t n_zeros, const double *A, cons
 int mb_polish_single_exact(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                            const double *delta, int64_t n_zeros, int weight_slot, double grid_hw, int grid_steps,
                            double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);
+/* polish_peaks_with_weights (search/path1_eval_fast.cpp:58-143: h0; grid of 2 grid_steps + 1
+ * shifts over the first min(n, 4096) zeros; <= 6 Newton steps, clamp 1e-4) for every candidate,
+ * with (A_j, B_j) computed on the fly as in mb_exact_AB instead of read from P x N matrices:
+ * the search drivers' compute_peak_AB + polish per weight vector (search/eval_tech1_600k.py:216-273)
+ * without the matrices. */
+int mb_polish_peaks_exact(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                          const double *delta, int64_t n_zeros, int weight_slot, double grid_half_width,
+                          int grid_steps, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);
 int mb_fast_polish_exact(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                          const double *delta, int64_t n_zeros, int weight_slot, const double *ddy_grid,
                          int64_t n_grid, int top, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);

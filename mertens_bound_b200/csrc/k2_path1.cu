@@ -5,6 +5,8 @@
 //                                         mb_polish_single_exact (A/B computed on the fly)
 //   fast_polish_batch_blas  (:150-221) -> mb_fast_polish_batch (A/B rows) and
 //                                         mb_fast_polish_exact (A/B computed on the fly)
+// and, for the search drivers' polish_peaks_with_weights (search/path1_eval_fast.cpp:58-143, whose
+// A/B form is in k2_compat.cu), mb_polish_peaks_exact with (A, B) computed on the fly.
 // The *_exact forms read the table and the peaks' 64.64 fixed-point v (+ delta) and never form the
 // P x N matrices, so they are bound by the phase and sincos work, not by 16 B/term of HBM traffic.
 #include <algorithm>
@@ -281,6 +283,27 @@ extern "C" int mb_polish_single_exact(mb_table *h, int64_t P, const uint64_t *v_
     MB_TRY(stage_exact(t, P, v_int, v_frac, delta, grid.data(), (int64_t)grid.size(), 0, s));
     PolishArgs a{n_zeros, t.d_gamma, t.d_weights[weight_slot], s.grid, (int)grid.size(), 0.0, nullptr, s.hu, s.hp, s.dp};
     peak_polish_kernel<ABExact, POLISH_SINGLE><<<(unsigned)P, POLISH_THREADS, 0, t.stream>>>(
+        ABExact{view(t), s.vi, s.vf, s.delta}, a);
+    MB_CUDA(cudaGetLastError());
+    return fetch_outputs(t.stream, P, s.hu, s.hp, s.dp, out_h_unpol, out_h_pol, out_ddy_pol);
+}
+
+extern "C" int mb_polish_peaks_exact(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                                     const double *delta, int64_t n_zeros, int weight_slot, double grid_half_width,
+                                     int grid_steps, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol) {
+    const char *who = "mb_polish_peaks_exact";
+    MB_CHECK_ARG(h && out_h_unpol && out_h_pol && out_ddy_pol, "%s: null argument", who);
+    Table &t = table_of(h);
+    MB_TRY(check_peaks(t, P, v_int, v_frac, delta, n_zeros, who));
+    MB_TRY(check_weights(t, weight_slot, who));
+    MB_CHECK_ARG(grid_steps >= 0 && grid_steps <= (1 << 19) && std::isfinite(grid_half_width), "%s: bad grid", who);
+    if (P == 0) return MB_OK;
+    MB_TRY(device_guard(t.device));
+    ExactStage s;
+    MB_TRY(stage_exact(t, P, v_int, v_frac, delta, nullptr, 0, 0, s));
+    PolishArgs a{n_zeros, t.d_gamma, t.d_weights[weight_slot], nullptr, grid_steps, grid_half_width, nullptr,
+                 s.hu, s.hp, s.dp};
+    peak_polish_kernel<ABExact, POLISH_EVAL_FAST><<<(unsigned)P, POLISH_THREADS, 0, t.stream>>>(
         ABExact{view(t), s.vi, s.vf, s.delta}, a);
     MB_CUDA(cudaGetLastError());
     return fetch_outputs(t.stream, P, s.hu, s.hp, s.dp, out_h_unpol, out_h_pol, out_ddy_pol);

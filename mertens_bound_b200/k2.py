@@ -10,6 +10,7 @@ Candidates are 64.64 fixed point (v_int, v_frac) plus an FP64 offset delta
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 import math
 
 import numpy as np
@@ -64,8 +65,13 @@ class ZeroTable:
         w = _f64(w)
         if w.shape != (self.n,):
             raise ValueError(f"weights must have shape ({self.n},)")
+        key = hashlib.sha1(w.tobytes()).hexdigest()      # a vector registered before keeps its slot
+        cache = self.__dict__.setdefault("_weight_slots", {})
+        if key in cache:
+            return cache[key]
         slot = C.c_int()
         check(_lib.lib().mb_table_add_weights(self.handle, ptr(w), self.n, C.byref(slot)))
+        cache[key] = slot.value
         return slot.value
 
     def count_below(self, T: float) -> int:

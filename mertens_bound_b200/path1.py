@@ -12,6 +12,7 @@ and never form the P x N matrices:
     slot = table.add_weights(w)
     h0, h, ddy = polish_single_exact(table, cands, slot, n_zeros)
     h_unpol, h_pol, ddy_pol = fast_polish_exact(table, cands, slot, n_zeros)
+    h_unpol, h_pol, ddy_pol = polish_peaks_exact(table, cands, slot, n_zeros)   # path1_eval_fast.cpp:58
 
 Errors raise K2Error.  A peak is y = v + delta, v in 64.64 fixed point
 (mertens_bound_b200.synth.Candidates).
@@ -113,4 +114,17 @@ def fast_polish_exact(table, cands, weight_slot: int, n_zeros: int | None = None
     hu, hp, dp = np.empty(P), np.empty(P), np.empty(P)
     check(_lib.lib().mb_fast_polish_exact(table.handle, P, ptr(vi), ptr(vf), ptr(d), n, int(weight_slot),
                                           ptr(grid), grid.shape[0], int(top), ptr(hu), ptr(hp), ptr(dp)))
+    return hu, hp, dp
+
+
+def polish_peaks_exact(table, cands, weight_slot: int, n_zeros: int | None = None,
+                       grid_half_width: float = 2.5e-4, grid_steps: int = 40):
+    """polish_peaks_with_weights (search/path1_eval_fast.cpp:58-143) for every candidate, (A, B)
+    computed on the fly; the defaults are the search drivers' settings (eval_tech1_600k.py:262)."""
+    vi, vf, d = _cands(cands)
+    P = vi.shape[0]
+    n = table.n if n_zeros is None else int(n_zeros)
+    hu, hp, dp = np.empty(P), np.empty(P), np.empty(P)
+    check(_lib.lib().mb_polish_peaks_exact(table.handle, P, ptr(vi), ptr(vf), ptr(d), n, int(weight_slot),
+                                           float(grid_half_width), int(grid_steps), ptr(hu), ptr(hp), ptr(dp)))
     return hu, hp, dp
