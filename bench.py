@@ -475,6 +475,43 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
             gain = float((h4[1].abs() - h4[0].abs()).mean())
         out["newton_polish"] = {"zero_terms_per_eval": terms, "eval_ms": em, "eval_rate": terms / em * 1e3,
                                 "newton8_ms": nm, "evals_per_newton": 10, "mean_abs_gain": gain}
+
+    # driver_scoring: the search drivers' step (search/eval_tech1_600k.py:216-273) -- 256
+    # candidates over the first 600,000 zeros, polish_peaks_with_weights under the five weight
+    # vectors -- matrix-free on the GPU; beside it the reference's compiled evaluator
+    # (compute_peak_AB once + five polishes) on 16 of the candidates
+    from mertens_bound_b200 import score
+    d600 = big.truncate(600_000)
+    c6 = synth.make_candidates(256, seed=6)
+    c6.delta[:] = np.random.default_rng(6).uniform(-1e-4, 1e-4, 256)
+    W = score.reference_weights(d600.gamma)
+    with k2.ZeroTable.from_data(d600, device=dev.index) as t6:
+        score.score(t6, c6.subset(np.arange(8)), W)                       # registers the vectors
+        t0 = time.perf_counter()
+        res = score.score(t6, c6, W)
+        gpu_s = time.perf_counter() - t0
+    ds = {"candidates": 256, "zeros": 600_000, "weights": list(W), "grid": "2.5e-4 / 40 steps",
+          "seconds": gpu_s, "candidates_per_s": 256 / gpu_s,
+          "best_abs_h_pol": float(max(np.max(np.abs(v[1])) for v in res.values()))}
+    if cpu_baseline:
+        try:
+            from oracle.oracle import RefLib, reference_candidates, reference_format
+            if RefLib.available():
+                R = RefLib()
+                sub = c6.subset(np.arange(16))
+                reft = reference_format(d600, exact_psi=False)
+                t0 = time.perf_counter()
+                A, B = R.peak_AB(reference_candidates(sub), reft)
+                for w in W.values():
+                    R.polish(A, B, d600.gamma, w, 2.5e-4, 40)
+                cs = time.perf_counter() - t0
+                ds["cpu_baseline"] = {"kind": "reference", "cores": 16, "candidates": 16, "seconds": cs,
+                                      "candidates_per_s": 16 / cs,
+                                      "sample": "compute_peak_AB + 5 x polish_peaks_with_weights, "
+                                                "search/path1_eval_fast.cpp compiled in oracle/_ref"}
+        except Exception as e:                                       # the baseline is optional
+            ds["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    out["driver_scoring"] = ds
     return out
 
 
