@@ -121,3 +121,24 @@ def test_tail_skip_within_bound(gpu, oracle):
         assert plan.group_info(0)["n_eval"] == data.n
         again, _, _ = plan.run(cd)
         assert np.array_equal(again, full)
+
+
+def test_plan_ragged_and_empty_groups(table, small_table):
+    """Groups with no candidates, with no zeros below T (the sum is 0), and with one candidate."""
+    counts = [0, 17, 0, 33, 1, 5]
+    ks = [3e-9, 1e-9, 3e-9, 3e-9, 1.5e-10, 3e-9]
+    Ts = [math.inf, 5000.0, 100.0, 10.0, math.inf, 14.0]     # gamma_1 ~ 14.13: T = 10, 14 keep none
+    cd = synth.make_candidates(sum(counts), seed=12)
+    with k2.Plan(table, counts, ks, Ts, tol=TOL) as plan:
+        val, dd, dk = plan.run(cd)
+        off = 0
+        for g, (c, kk, TT) in enumerate(zip(counts, ks, Ts)):
+            if c == 0:
+                continue
+            sub = cd.subset(np.arange(off, off + c))
+            pv, _, _ = k2.k2_plain(table, sub, kk, TT)
+            gi = plan.group_info(g)
+            if gi["n_T"] == 0:
+                assert np.all(val[off:off + c] == 0) and np.all(pv == 0)
+            assert np.max(np.abs(val[off:off + c] - pv)) <= gi["err_bound"] + 1e-15
+            off += c
