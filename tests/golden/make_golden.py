@@ -9,7 +9,8 @@ small_plain.json    64 candidates x 10,000 synthetic zeros (table seed 1, candid
                         (polish_peaks_with_weights with grid_steps = 0) and its polished h/ddy with
                         the drivers' settings (grid_half_width 2.5e-4, 40 steps);
                       * the binary128 oracle's K2, dK2/ddelta, dK2/dk (hi + lo doubles);
-                      * mpmath interval balls of K2 for 4 candidates (220 bits);
+                      * mpmath interval balls of K2 and of dK2/ddelta, dK2/dk for 4 candidates
+                        (220 bits);
                       * exact phases floor(frac(v G) 2^128) for 16 (candidate, zero) pairs.
 peak2_full_ball.json the interval ball of K2 at the reference's Peak2 point over all 2,325,572
                     synthetic zeros below 1.3e6 (table seed 1), k = 1.5e-10, as exact rational
@@ -78,12 +79,14 @@ def small_fixture():
         out["reference_evaluator"] = {"h0": [float(x) for x in h0], "h_pol": [float(x) for x in hp],
                                       "ddy_pol": [float(x) for x in dp],
                                       "source": "search/path1_eval_fast.cpp compiled by oracle/Makefile"}
-    balls = []
+    balls, dballs = [], []
     for p in range(4):
-        val, _, _ = k2_ball(c.v_int[p], c.v_frac[p], 0.0, t.G3, t.c_re, t.c_im, k, t.n)
+        val, dd, dk = k2_ball(c.v_int[p], c.v_frac[p], 0.0, t.G3, t.c_re, t.c_im, k, t.n)
         a, b = bounds(val)
         balls.append([frac_str(a), frac_str(b)])
+        dballs.append({"dd": [frac_str(x) for x in bounds(dd)], "dk": [frac_str(x) for x in bounds(dk)]})
     out["interval_balls_first4"] = balls
+    out["derivative_balls_first4"] = dballs
     pairs = []
     rng = np.random.default_rng(7)
     for _ in range(16):

@@ -74,6 +74,21 @@ def test_interval_balls_contain_oracle(small):
         assert Fraction(b) - Fraction(a) < Fraction(1, 10 ** 30)
 
 
+def test_derivative_balls_contain_oracle(small):
+    """dK2/ddelta and dK2/dk of the binary128 oracle inside the 220-bit interval derivatives."""
+    fx, t, c = small
+    if "derivative_balls_first4" not in fx:
+        pytest.skip("fixture made without derivative balls")
+    for p, balls in enumerate(fx["derivative_balls_first4"]):
+        for key in ("dd", "dk"):
+            a, b = (Fraction(x) for x in balls[key])
+            hi, lo = fx["oracle_k2"][key][p]
+            x = Fraction(hi) + Fraction(lo)
+            slack = abs(x) * Fraction(1, 10 ** 28)
+            assert a - slack <= x <= b + slack, (p, key)
+            assert b - a <= abs(x) * Fraction(1, 10 ** 40)
+
+
 def test_exact_phases(small, oracle):
     fx, t, c = small
     for e in fx["exact_phases"]:
@@ -100,8 +115,15 @@ def test_kernels_against_fixture(gpu, small):
         val, dd, dk = k2.k2_plain(tb, c, fx["k"])
         want = np.array(fx["oracle_k2"]["val"])[:, 0]
         assert np.max(np.abs(val - want)) < 2e-13
-        fv, _, _, eb = k2.k2_fast(tb, c, fx["k"])
+        fv, fd, fk, eb = k2.k2_fast(tb, c, fx["k"])
         assert np.max(np.abs(fv - want)) <= eb <= 1e-10
+        # derivatives against the 220-bit interval derivatives (the "Arb derivative")
+        for p, balls in enumerate(fx.get("derivative_balls_first4", [])):
+            for key, plain_v, fast_v in (("dd", dd[p], fd[p]), ("dk", dk[p], fk[p])):
+                a, b = (float(Fraction(x)) for x in balls[key])
+                mid = 0.5 * (a + b)
+                assert abs(plain_v - mid) <= 1e-10 * abs(mid), (p, key)
+                assert abs(fast_v - mid) <= 1e-6 * abs(mid), (p, key)
         lo, hi, _ = k2.k2_certified(tb, c.subset(np.arange(4)), fx["k"])
         for p, (a, b) in enumerate(fx["interval_balls_first4"]):
             assert Fraction(lo[p]) <= Fraction(a) and Fraction(b) <= Fraction(hi[p])
