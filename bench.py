@@ -61,11 +61,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="skip the summary of the other workloads")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--profile-case", choices=["small", "search"], default=None,
+    ap.add_argument("--profile-case", choices=["small", "search", "extras"], default=None,
                     help="run a fixed case for ncu captures (no timing): 'small' = zeros below 1e5 x "
                          "2,048 candidates, all kernels of one plan run; 'search' = the bench workload, "
                          "each kernel launched alone once (plain; light tier at 2, 3, 4 candidates per "
-                         "thread; heavy tier)")
+                         "thread; heavy tier); 'extras' = certified, screen and polish kernels once each")
     return ap.parse_args()
 
 
@@ -558,6 +558,26 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_extras():
+    """One launch each of the kernels beside the tiers, at modest sizes (~0.5 GB on the device):
+    the certified interval over all 2,325,572 zeros at the Peak2 point, the leaf screen (4,096
+    leaves, 64/128/256 zeros), polish_peaks_with_weights matrix-free (32 candidates x 100,000
+    zeros) and the Taylor-moment polish matrix-free (256 candidates x 100,000 zeros)."""
+    from mertens_bound_b200 import hit_polish, k2, path1, synth
+    big = synth.make_table(2_325_572, seed=1)
+    with k2.ZeroTable.from_data(big) as tb:
+        k2.k2_certified(tb, synth.peak2_candidate(), 1.5e-10, 1.3e6, v_rad=2.0 ** -64)
+    d = big.truncate(100_000)
+    c = synth.make_candidates(4096, seed=9)
+    with k2.ZeroTable.from_data(d) as t:
+        pts = np.stack([c.v_int, c.v_frac], axis=1)
+        r = hit_polish.screen_leaves(t, pts, 3e-9, hit_polish.SCREEN_GPU)
+        slot = t.add_weights(np.exp(-3e-9 * d.gamma * d.gamma))
+        path1.polish_peaks_exact(t, c.subset(np.arange(32)), slot)
+        path1.fast_polish_exact(t, c.subset(np.arange(256)), slot)
+    print(json.dumps({"profile_case": "extras", "screen_hits": int(len(r.hits))}), flush=True)
+
+
 def run_profile_case(args):
     """Fixed cases for ncu captures (no timing, no bench line).
       small   zeros below 1e5, 2,048 candidates: the chosen form (light tier at 4 candidates per
@@ -565,6 +585,8 @@ def run_profile_case(args):
               device);
       search  the bench workload (zeros below 3e5, 4,096 candidates): the plain kernel once, the
               light tier alone at 2, 3 and 4 candidates per thread, the heavy tier alone (~80 MB)."""
+    if args.profile_case == "extras":
+        return run_profile_extras()
     import torch
     from mertens_bound_b200 import k2, synth, _lib
     from mertens_bound_b200._lib import check
