@@ -165,7 +165,7 @@ extern "C" int mb_polish_peaks_with_weights(int n_peaks, int n_zeros, const doub
             MB_CUDA(cudaMemcpyAsync(d_B, B + (size_t)p0 * n_zeros, (size_t)np * n_zeros * 8, cudaMemcpyHostToDevice, s));
         }
         PolishArgs a{n_zeros, d_g, d_w, nullptr, grid_steps, grid_half_width, nullptr, d_hu, d_hp, d_dp};
-        peak_polish_kernel<ABMatrix, POLISH_EVAL_FAST><<<np, POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, a);
+        peak_polish_kernel<ABMatrix, POLISH_EVAL_FAST><<<(unsigned)(np * POLISH_CLUSTER), POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, a);
         MB_CUDA(cudaGetLastError());
         MB_CUDA(cudaMemcpyAsync(out_h_unpol + p0, d_hu, np * 8, cudaMemcpyDeviceToHost, s));
         MB_CUDA(cudaMemcpyAsync(out_h_pol + p0, d_hp, np * 8, cudaMemcpyDeviceToHost, s));

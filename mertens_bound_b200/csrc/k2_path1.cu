@@ -19,6 +19,9 @@
 namespace mb {
 namespace {
 
+// one cluster of POLISH_CLUSTER CTAs per peak: the grid stays within 2^31 - 1 CTAs
+constexpr int64_t MAX_POLISH_PEAKS = (int64_t)1 << 26;
+
 __global__ void exact_ab_kernel(ABExact src, int64_t n, int64_t p0, double *A, double *B) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -191,7 +194,7 @@ extern "C" int mb_polish_single_peak(int64_t n_peaks, int64_t n_zeros, int64_t l
             MB_CUDA(cudaMemcpy2DAsync(d_B, n_zeros * 8, B + p0 * ld, ld * 8, n_zeros * 8, np, cudaMemcpyHostToDevice, s));
         }
         PolishArgs a{n_zeros, d_g, d_w, d_grid, (int)grid.size(), 0.0, nullptr, d_hu, d_hp, d_dp};
-        peak_polish_kernel<ABMatrix, POLISH_SINGLE><<<(unsigned)np, POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, a);
+        peak_polish_kernel<ABMatrix, POLISH_SINGLE><<<(unsigned)(np * POLISH_CLUSTER), POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, a);
         MB_CUDA(cudaGetLastError());
         MB_CUDA(cudaMemcpyAsync(out_h_unpol + p0, d_hu, np * 8, cudaMemcpyDeviceToHost, s));
         MB_CUDA(cudaMemcpyAsync(out_h_pol + p0, d_hp, np * 8, cudaMemcpyDeviceToHost, s));
@@ -234,7 +237,7 @@ extern "C" int mb_fast_polish_batch(int64_t n_peaks, int64_t n_zeros, const doub
             MB_CUDA(cudaMemcpyAsync(d_B, B + p0 * N, np * N * 8, cudaMemcpyHostToDevice, s));
         }
         MomentArgs m{n_zeros, d_g, d_w, d_grid, (int)n_grid, d_hu + p0, d_hp + p0, d_dp + p0};
-        taylor_moments_kernel<ABMatrix><<<(unsigned)np, POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, m);
+        taylor_moments_kernel<ABMatrix><<<(unsigned)(np * POLISH_CLUSTER), POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, m);
         MB_CUDA(cudaGetLastError());
     }
     MB_TRY(fetch_outputs(s, n_peaks, d_hu, d_hp, d_dp, out_h_unpol, out_h_pol, out_ddy_pol));
@@ -253,7 +256,7 @@ extern "C" int mb_fast_polish_batch(int64_t n_peaks, int64_t n_zeros, const doub
             MB_CUDA(cudaMemcpyAsync(d_dp + r, out_ddy_pol + q, 8, cudaMemcpyHostToDevice, s));
         }
         PolishArgs a{n_zeros, d_g, d_w, nullptr, 0, 0.0, nullptr, d_hu, d_hp, d_dp};
-        peak_polish_kernel<ABMatrix, POLISH_TOPK><<<(unsigned)np, POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, a);
+        peak_polish_kernel<ABMatrix, POLISH_TOPK><<<(unsigned)(np * POLISH_CLUSTER), POLISH_THREADS, 0, s>>>(ABMatrix{d_A, d_B, n_zeros}, a);
         MB_CUDA(cudaGetLastError());
         std::vector<double> hp(np), dp(np);
         MB_CUDA(cudaMemcpyAsync(hp.data(), d_hp, np * 8, cudaMemcpyDeviceToHost, s));
@@ -272,6 +275,8 @@ extern "C" int mb_polish_single_exact(mb_table *h, int64_t P, const uint64_t *v_
                                       int grid_steps, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol) {
     const char *who = "mb_polish_single_exact";
     MB_CHECK_ARG(h && out_h_unpol && out_h_pol && out_ddy_pol, "%s: null argument", who);
+    MB_CHECK_ARG(P <= MAX_POLISH_PEAKS, "%s: P=%lld above %lld peaks per call", who, (long long)P,
+                 (long long)MAX_POLISH_PEAKS);
     Table &t = table_of(h);
     MB_TRY(check_peaks(t, P, v_int, v_frac, delta, n_zeros, who));
     MB_TRY(check_weights(t, weight_slot, who));
@@ -282,7 +287,7 @@ extern "C" int mb_polish_single_exact(mb_table *h, int64_t P, const uint64_t *v_
     ExactStage s;
     MB_TRY(stage_exact(t, P, v_int, v_frac, delta, grid.data(), (int64_t)grid.size(), 0, s));
     PolishArgs a{n_zeros, t.d_gamma, t.d_weights[weight_slot], s.grid, (int)grid.size(), 0.0, nullptr, s.hu, s.hp, s.dp};
-    peak_polish_kernel<ABExact, POLISH_SINGLE><<<(unsigned)P, POLISH_THREADS, 0, t.stream>>>(
+    peak_polish_kernel<ABExact, POLISH_SINGLE><<<(unsigned)(P * POLISH_CLUSTER), POLISH_THREADS, 0, t.stream>>>(
         ABExact{view(t), s.vi, s.vf, s.delta}, a);
     MB_CUDA(cudaGetLastError());
     return fetch_outputs(t.stream, P, s.hu, s.hp, s.dp, out_h_unpol, out_h_pol, out_ddy_pol);
@@ -293,6 +298,8 @@ extern "C" int mb_polish_peaks_exact(mb_table *h, int64_t P, const uint64_t *v_i
                                      int grid_steps, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol) {
     const char *who = "mb_polish_peaks_exact";
     MB_CHECK_ARG(h && out_h_unpol && out_h_pol && out_ddy_pol, "%s: null argument", who);
+    MB_CHECK_ARG(P <= MAX_POLISH_PEAKS, "%s: P=%lld above %lld peaks per call", who, (long long)P,
+                 (long long)MAX_POLISH_PEAKS);
     Table &t = table_of(h);
     MB_TRY(check_peaks(t, P, v_int, v_frac, delta, n_zeros, who));
     MB_TRY(check_weights(t, weight_slot, who));
@@ -303,7 +310,7 @@ extern "C" int mb_polish_peaks_exact(mb_table *h, int64_t P, const uint64_t *v_i
     MB_TRY(stage_exact(t, P, v_int, v_frac, delta, nullptr, 0, 0, s));
     PolishArgs a{n_zeros, t.d_gamma, t.d_weights[weight_slot], nullptr, grid_steps, grid_half_width, nullptr,
                  s.hu, s.hp, s.dp};
-    peak_polish_kernel<ABExact, POLISH_EVAL_FAST><<<(unsigned)P, POLISH_THREADS, 0, t.stream>>>(
+    peak_polish_kernel<ABExact, POLISH_EVAL_FAST><<<(unsigned)(P * POLISH_CLUSTER), POLISH_THREADS, 0, t.stream>>>(
         ABExact{view(t), s.vi, s.vf, s.delta}, a);
     MB_CUDA(cudaGetLastError());
     return fetch_outputs(t.stream, P, s.hu, s.hp, s.dp, out_h_unpol, out_h_pol, out_ddy_pol);
@@ -315,6 +322,8 @@ extern "C" int mb_fast_polish_exact(mb_table *h, int64_t P, const uint64_t *v_in
                                     double *out_ddy_pol) {
     const char *who = "mb_fast_polish_exact";
     MB_CHECK_ARG(h && out_h_unpol && out_h_pol && out_ddy_pol, "%s: null argument", who);
+    MB_CHECK_ARG(P <= MAX_POLISH_PEAKS, "%s: P=%lld above %lld peaks per call", who, (long long)P,
+                 (long long)MAX_POLISH_PEAKS);
     Table &t = table_of(h);
     MB_TRY(check_peaks(t, P, v_int, v_frac, delta, n_zeros, who));
     MB_TRY(check_weights(t, weight_slot, who));
@@ -328,14 +337,14 @@ extern "C" int mb_fast_polish_exact(mb_table *h, int64_t P, const uint64_t *v_in
     const ABExact src{view(t), s.vi, s.vf, s.delta};
     const double *d_w = t.d_weights[weight_slot];
     MomentArgs m{n_zeros, t.d_gamma, d_w, s.grid, (int)n_grid, s.hu, s.hp, s.dp};
-    taylor_moments_kernel<ABExact><<<(unsigned)P, POLISH_THREADS, 0, t.stream>>>(src, m);
+    taylor_moments_kernel<ABExact><<<(unsigned)(P * POLISH_CLUSTER), POLISH_THREADS, 0, t.stream>>>(src, m);
     MB_CUDA(cudaGetLastError());
     MB_TRY(fetch_outputs(t.stream, P, s.hu, s.hp, s.dp, out_h_unpol, out_h_pol, out_ddy_pol));
     if (nsel == 0) return MB_OK;
     const std::vector<int> sel = top_indices(out_h_pol, P, nsel);
     MB_CUDA(cudaMemcpyAsync(s.sel, sel.data(), nsel * sizeof(int), cudaMemcpyHostToDevice, t.stream));
     PolishArgs a{n_zeros, t.d_gamma, d_w, nullptr, 0, 0.0, s.sel, s.hu, s.hp, s.dp};
-    peak_polish_kernel<ABExact, POLISH_TOPK><<<(unsigned)nsel, POLISH_THREADS, 0, t.stream>>>(src, a);
+    peak_polish_kernel<ABExact, POLISH_TOPK><<<(unsigned)(nsel * POLISH_CLUSTER), POLISH_THREADS, 0, t.stream>>>(src, a);
     MB_CUDA(cudaGetLastError());
     return fetch_outputs(t.stream, P, s.hu, s.hp, s.dp, out_h_unpol, out_h_pol, out_ddy_pol);
 }

@@ -1,5 +1,8 @@
 // Per-peak polish of  h(ddy) = sum_j w_j (A_j cos(gamma_j ddy) - B_j sin(gamma_j ddy)),
-// one CTA per peak (the sequential steps of the reference loops become block-wide reductions).
+// one thread-block cluster of POLISH_CLUSTER CTAs per peak: each CTA sums a stride of the zeros,
+// and the sequential steps of the reference loops become cluster-wide reductions through
+// distributed shared memory (every CTA adds the CTA totals in rank order, so all CTAs hold the
+// same bits and take the same branches).  A handful of peaks thus spreads over 8x as many SMs.
 //
 // (A_j, B_j) = 2 c_j e^{i gamma_j y} of a peak come from a source:
 //   ABMatrix  rows of caller matrices (the reference's A/B contract, search/path1_eval_fast.cpp:15-53,
@@ -7,12 +10,16 @@
 //   ABExact   computed on the fly from the exact 128-bit phase of the peak's v (+ delta), so no
 //             P x N matrix is written or read.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "k2_common.cuh"
 #include "k2_internal.h"
 
 namespace mb {
 
 constexpr int POLISH_THREADS = 256;
+constexpr int POLISH_CLUSTER = 8;     // CTAs per peak (portable cluster size)
+constexpr int64_t POLISH_STRIDE = (int64_t)POLISH_CLUSTER * POLISH_THREADS;
 
 // Sum over the CTA; every thread gets the result.  Warp partials are added in warp order, so the
 // result does not depend on scheduling.
@@ -27,6 +34,30 @@ __device__ __forceinline__ double block_sum(double x, double *red) {
     for (int w = 0; w < POLISH_THREADS / 32; ++w) s += red[w];
     return s;
 }
+
+// The calling thread's place in its peak's cluster and the cluster-wide sum.
+struct Team {
+    int64_t first;         // rank * POLISH_THREADS + threadIdx.x: first zero of this thread
+    double *red;           // CTA scratch of block_sum
+    double *slot;          // this CTA's two exchange slots (double-buffered)
+    int parity;
+
+    // Sum of x over all threads of the cluster; every thread of every CTA gets the same value.
+    // One cluster barrier per call: a CTA rewrites a slot only after the barrier of the next
+    // call, which every peer reaches after reading it.
+    __device__ double sum(double x) {
+        const double s = block_sum(x, red);
+        namespace cg = cooperative_groups;
+        cg::cluster_group cl = cg::this_cluster();
+        if (threadIdx.x == 0) slot[parity] = s;
+        cl.sync();
+        double t = 0.0;
+#pragma unroll
+        for (int r = 0; r < POLISH_CLUSTER; ++r) t += *cl.map_shared_rank(&slot[parity], r);
+        parity ^= 1;
+        return t;
+    }
+};
 
 struct ABMatrix {
     const double *A, *B;
@@ -108,15 +139,15 @@ struct ABExact {
 // h at ddy (all threads get it).
 template <class Src>
 __device__ double polish_h(const Src &src, const typename Src::Peak &pk, int64_t n, const double *gamma,
-                           const double *w, double ddy, double *red) {
+                           const double *w, double ddy, Team &tm) {
     double h = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += POLISH_THREADS) {
+    for (int64_t i = tm.first; i < n; i += POLISH_STRIDE) {
         double a, b, sn, cs;
         src.at(pk, i, a, b);
         sincos(gamma[i] * ddy, &sn, &cs);
         h += w[i] * (a * cs - b * sn);
     }
-    return block_sum(h, red);
+    return tm.sum(h);
 }
 
 // Newton on h'(ddy) = 0 from ddy: at most `iters` steps, each clamped to +-clamp; stops after a
@@ -125,10 +156,10 @@ __device__ double polish_h(const Src &src, const typename Src::Peak &pk, int64_t
 template <class Src>
 __device__ double polish_newton(const Src &src, const typename Src::Peak &pk, int64_t n, const double *gamma,
                                 const double *w, double ddy, int iters, double clamp, double step_tol,
-                                double *red) {
+                                Team &tm) {
     for (int it = 0; it < iters; ++it) {
         double fp = 0.0, fpp = 0.0;
-        for (int64_t i = threadIdx.x; i < n; i += POLISH_THREADS) {
+        for (int64_t i = tm.first; i < n; i += POLISH_STRIDE) {
             const double g = gamma[i];
             double a, b, sn, cs;
             src.at(pk, i, a, b);
@@ -138,8 +169,8 @@ __device__ double polish_newton(const Src &src, const typename Src::Peak &pk, in
             fp += w[i] * dval;
             fpp += w[i] * (-(g * g) * val);
         }
-        fp = block_sum(fp, red);
-        fpp = block_sum(fpp, red);
+        fp = tm.sum(fp);
+        fpp = tm.sum(fpp);
         if (!(fabs(fpp) > 1e-12)) break;
         double step = fp / fpp;
         step = fmin(fmax(step, -clamp), clamp);
@@ -174,80 +205,91 @@ struct PolishArgs {
     double *h_unpol, *h_pol, *ddy_pol;
 };
 
+// Grid: POLISH_CLUSTER CTAs per peak (cluster c serves peak sel[c], or c).  Rank 0 writes the
+// results; every CTA waits at a last cluster barrier so none exits while a peer may still read
+// its exchange slots.
 template <class Src, int MODE>
-__global__ void __launch_bounds__(POLISH_THREADS) peak_polish_kernel(Src src, PolishArgs a) {
+__global__ void __cluster_dims__(POLISH_CLUSTER, 1, 1) __launch_bounds__(POLISH_THREADS)
+    peak_polish_kernel(Src src, PolishArgs a) {
     __shared__ double red[POLISH_THREADS / 32];
-    const int64_t p = a.sel ? a.sel[blockIdx.x] : blockIdx.x;
+    __shared__ double slot[2];
+    namespace cg = cooperative_groups;
+    const int rank = (int)cg::this_cluster().block_rank();
+    const int64_t cid = blockIdx.x / POLISH_CLUSTER;
+    Team tm{(int64_t)rank * POLISH_THREADS + threadIdx.x, red, slot, 0};
+    const bool writer = rank == 0 && threadIdx.x == 0;
+    const int64_t p = a.sel ? a.sel[cid] : cid;
     const typename Src::Peak pk = src.peak(p);
     const int64_t n = a.n;
     if (MODE == POLISH_TOPK) {
         const double hu = a.h_unpol[p];
-        const double ddy = polish_newton(src, pk, n, a.gamma, a.w, a.ddy_pol[p], 4, 1e-5, 1e-13, red);
-        const double h = polish_h(src, pk, n, a.gamma, a.w, ddy, red);
-        if (threadIdx.x == 0) {
+        const double ddy = polish_newton(src, pk, n, a.gamma, a.w, a.ddy_pol[p], 4, 1e-5, 1e-13, tm);
+        const double h = polish_h(src, pk, n, a.gamma, a.w, ddy, tm);
+        if (writer) {
             const bool better = fabs(h) > fabs(hu);
             a.h_pol[p] = better ? h : hu;
             a.ddy_pol[p] = better ? ddy : 0.0;
         }
-        return;
-    }
-    double s = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += POLISH_THREADS) {
-        double x, y;
-        src.at(pk, i, x, y);
-        s += a.w[i] * x;
-    }
-    const double h0 = block_sum(s, red);
-    if (MODE == POLISH_EVAL_FAST) {
-        const int steps = a.n_grid;
-        const int64_t k_scan = n < 4096 ? n : 4096;
-        double best_ddy = 0.0, best_abs = fabs(h0);
-        for (int m = -steps; m <= steps && steps > 0; ++m) {
-            const double ddy = (a.half * m) / steps;
-            const double hs = fabs(polish_h(src, pk, k_scan, a.gamma, a.w, ddy, red));
-            if (hs > best_abs) {
-                best_abs = hs;
-                best_ddy = ddy;
+    } else {
+        double s = 0.0;
+        for (int64_t i = tm.first; i < n; i += POLISH_STRIDE) {
+            double x, y;
+            src.at(pk, i, x, y);
+            s += a.w[i] * x;
+        }
+        const double h0 = tm.sum(s);
+        if (MODE == POLISH_EVAL_FAST) {
+            const int steps = a.n_grid;
+            const int64_t k_scan = n < 4096 ? n : 4096;
+            double best_ddy = 0.0, best_abs = fabs(h0);
+            for (int m = -steps; m <= steps && steps > 0; ++m) {
+                const double ddy = (a.half * m) / steps;
+                const double hs = fabs(polish_h(src, pk, k_scan, a.gamma, a.w, ddy, tm));
+                if (hs > best_abs) {
+                    best_abs = hs;
+                    best_ddy = ddy;
+                }
+            }
+            const double ddy = polish_newton(src, pk, n, a.gamma, a.w, best_ddy, 6, 1e-4, 1e-13, tm);
+            const double hf = polish_h(src, pk, n, a.gamma, a.w, ddy, tm);
+            if (writer) {
+                a.h_unpol[p] = h0;
+                const bool keep0 = fabs(h0) > fabs(hf);
+                a.h_pol[p] = keep0 ? h0 : hf;
+                a.ddy_pol[p] = keep0 ? 0.0 : ddy;
+            }
+        } else {  // POLISH_SINGLE
+            double best_h = h0, best_ddy = 0.0;
+            int n_starts = 1;
+            double grid_best = 0.0;
+            if (a.n_grid > 0) {
+                double top = -1.0;
+                for (int m = 0; m < a.n_grid; ++m) {
+                    const double hs = fabs(polish_h(src, pk, n, a.gamma, a.w, a.grid[m], tm));
+                    if (hs > top) {
+                        top = hs;
+                        grid_best = a.grid[m];
+                    }
+                }
+                n_starts = 2;
+            }
+            for (int st = 0; st < n_starts; ++st) {
+                const double ddy =
+                    polish_newton(src, pk, n, a.gamma, a.w, st == 0 ? 0.0 : grid_best, 8, 2e-5, 1e-14, tm);
+                const double h = polish_h(src, pk, n, a.gamma, a.w, ddy, tm);
+                if (fabs(h) > fabs(best_h)) {
+                    best_h = h;
+                    best_ddy = ddy;
+                }
+            }
+            if (writer) {
+                a.h_unpol[p] = h0;
+                a.h_pol[p] = best_h;
+                a.ddy_pol[p] = best_ddy;
             }
         }
-        const double ddy = polish_newton(src, pk, n, a.gamma, a.w, best_ddy, 6, 1e-4, 1e-13, red);
-        const double hf = polish_h(src, pk, n, a.gamma, a.w, ddy, red);
-        if (threadIdx.x == 0) {
-            a.h_unpol[p] = h0;
-            const bool keep0 = fabs(h0) > fabs(hf);
-            a.h_pol[p] = keep0 ? h0 : hf;
-            a.ddy_pol[p] = keep0 ? 0.0 : ddy;
-        }
-        return;
     }
-    // POLISH_SINGLE
-    double best_h = h0, best_ddy = 0.0;
-    int n_starts = 1;
-    double grid_best = 0.0;
-    if (a.n_grid > 0) {
-        double top = -1.0;
-        for (int m = 0; m < a.n_grid; ++m) {
-            const double hs = fabs(polish_h(src, pk, n, a.gamma, a.w, a.grid[m], red));
-            if (hs > top) {
-                top = hs;
-                grid_best = a.grid[m];
-            }
-        }
-        n_starts = 2;
-    }
-    for (int st = 0; st < n_starts; ++st) {
-        const double ddy = polish_newton(src, pk, n, a.gamma, a.w, st == 0 ? 0.0 : grid_best, 8, 2e-5, 1e-14, red);
-        const double h = polish_h(src, pk, n, a.gamma, a.w, ddy, red);
-        if (fabs(h) > fabs(best_h)) {
-            best_h = h;
-            best_ddy = ddy;
-        }
-    }
-    if (threadIdx.x == 0) {
-        a.h_unpol[p] = h0;
-        a.h_pol[p] = best_h;
-        a.ddy_pol[p] = best_ddy;
-    }
+    cg::this_cluster().sync();
 }
 
 // Degree-16 Taylor moments of h around ddy = 0 and their grid maximum
@@ -266,12 +308,17 @@ struct MomentArgs {
 };
 
 template <class Src>
-__global__ void __launch_bounds__(POLISH_THREADS) taylor_moments_kernel(Src src, MomentArgs a) {
+__global__ void __cluster_dims__(POLISH_CLUSTER, 1, 1) __launch_bounds__(POLISH_THREADS)
+    taylor_moments_kernel(Src src, MomentArgs a) {
     __shared__ double red[POLISH_THREADS / 32];
+    __shared__ double slot[2];
     __shared__ double mom[17];
     __shared__ double best_v[POLISH_THREADS], best_h[POLISH_THREADS];
     __shared__ int best_i[POLISH_THREADS];
-    const int64_t p = blockIdx.x;
+    namespace cg = cooperative_groups;
+    const int rank = (int)cg::this_cluster().block_rank();
+    Team tm{(int64_t)rank * POLISH_THREADS + threadIdx.x, red, slot, 0};
+    const int64_t p = blockIdx.x / POLISH_CLUSTER;
     const typename Src::Peak pk = src.peak(p);
     // (-1)^m/(2m)! and (-1)^m/(2m+1)!
     constexpr double CC[9] = {1.0, -1.0 / 2, 1.0 / 24, -1.0 / 720, 1.0 / 40320, -1.0 / 3628800,
@@ -283,7 +330,7 @@ __global__ void __launch_bounds__(POLISH_THREADS) taylor_moments_kernel(Src src,
     for (int m = 0; m < 9; ++m) c[m] = 0.0;
 #pragma unroll
     for (int m = 0; m < 8; ++m) s[m] = 0.0;
-    for (int64_t i = threadIdx.x; i < a.n; i += POLISH_THREADS) {
+    for (int64_t i = tm.first; i < a.n; i += POLISH_STRIDE) {
         double x, y;
         src.at(pk, i, x, y);
         const double u = a.gamma[i] * 1.0e-4, u2 = u * u;
@@ -298,15 +345,16 @@ __global__ void __launch_bounds__(POLISH_THREADS) taylor_moments_kernel(Src src,
     }
 #pragma unroll
     for (int m = 0; m < 9; ++m) {
-        const double v = block_sum(c[m], red);
+        const double v = tm.sum(c[m]);
         if (threadIdx.x == 0) mom[m] = v;
     }
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-        const double v = block_sum(s[m], red);
+        const double v = tm.sum(s[m]);
         if (threadIdx.x == 0) mom[9 + m] = v;
     }
-    __syncthreads();
+    cg::this_cluster().sync();      // peers are done reading this CTA's slots; mom[] visible
+    if (rank != 0) return;          // the grid search and the writes are rank 0's
     double bv = -1.0, hv = 0.0;
     int bi = -1;
     for (int g = threadIdx.x; g < a.n_grid; g += POLISH_THREADS) {
