@@ -149,6 +149,10 @@ int mb_plan_destroy(mb_plan *p);
  * derivative outputs omit the same zeros.  0 (the default) evaluates every zero below T, as the
  * reference does.  No reference counterpart (it sums every zero below its cutoff). */
 int mb_plan_set_skip(mb_plan *p, double skip_frac);
+/* A-priori bounds of the absolute error of group g's outputs: K2 (the bound of
+ * mb_plan_group_info), dK2/ddelta and dK2/dk (the same per-term errors applied to the amplitude
+ * sums 2|c| w gamma and 2|c| w gamma^2, plus the skipped zeros' sums under a tail skip). */
+int mb_plan_group_bounds(const mb_plan *p, int g, double *val, double *dd, double *dk);
 /* Zeros evaluated for group g (count_below(T) without a tail skip). */
 int mb_plan_group_zeros(const mb_plan *p, int g, int64_t *n_eval);
 /* Override the tile shape of group g: cpt in {1,2,4} candidates per thread, nzw in {1,2,4,8}

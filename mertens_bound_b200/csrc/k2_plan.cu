@@ -24,6 +24,7 @@ struct mb_plan {
     std::vector<int64_t> n_T, n_eval, n_heavy;   // zeros below T, zeros evaluated, heavy zeros
     double skip_frac = 0.0;        // share of tol given to skipping the tail of each group
     std::vector<double> err_bound, sum_abs;
+    std::vector<double> err_dd, err_dk;   // the same a-priori bounds for dK2/ddelta and dK2/dk
     std::vector<int> shape_nzw;
     std::vector<int64_t> heavy_chunk, light_chunk;
     int light_cpt = 4;
@@ -81,7 +82,7 @@ int default_nzw(int64_t P, int cpt) {
 //   n_h:    the smallest n_h with EPS_LIGHT * sum_{n_h <= j < n_eval} a_j <= (1/2 - skip_frac) tol.
 // Returns the a-priori bound of |K2 error| (skipped sum + tier errors + FP64 roundings).
 void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, double tol, double skip_frac,
-                int64_t &n_eval, int64_t &n_h, double &bound, double &sabs) {
+                int64_t &n_eval, int64_t &n_h, double &bound, double &sabs, double &bound_dd, double &bound_dk) {
     std::vector<double> a(n_use);
     double total = 0;
     for (int64_t j = 0; j < n_use; ++j) {
@@ -111,6 +112,17 @@ void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, doub
     // ~(terms per thread + chunks) roundings of 2^-53 relative; 1e-13 relative is a safe cover.
     bound = skipped + EPS_LIGHT * tail + EPS_HEAVY * heavy + 1e-13 * evaluated;
     sabs = total;
+    // the derivative terms are the value terms with amplitudes a gamma and a gamma^2 (computed
+    // the same way in each tier), so the same per-unit errors apply to those amplitude sums
+    double s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0};       // [heavy, light, skipped]
+    for (int64_t j = 0; j < n_use; ++j) {
+        const int tier = j < n_h ? 0 : (j < n_eval ? 1 : 2);
+        const double g = t.h_gamma[j];
+        s1[tier] += a[j] * g;
+        s2[tier] += a[j] * g * g;
+    }
+    bound_dd = s1[2] + EPS_LIGHT * s1[1] + EPS_HEAVY * s1[0] + 1e-13 * (s1[0] + s1[1]);
+    bound_dk = s2[2] + EPS_LIGHT * s2[1] + EPS_HEAVY * s2[0] + 1e-13 * (s2[0] + s2[1]);
 }
 
 void replan_tiers(mb_plan *p) {
@@ -118,7 +130,7 @@ void replan_tiers(mb_plan *p) {
     for (int g = 0; g < p->n_groups; ++g) {
         const double *wh = p->wslot[g] >= 0 ? t.h_weights[p->wslot[g]].data() : nullptr;
         plan_tiers(t, p->n_T[g], p->ks[g], wh, p->tol, p->skip_frac, p->n_eval[g], p->n_heavy[g],
-                   p->err_bound[g], p->sum_abs[g]);
+                   p->err_bound[g], p->sum_abs[g], p->err_dd[g], p->err_dk[g]);
     }
 }
 
@@ -298,6 +310,8 @@ extern "C" int mb_plan_create_weighted(mb_table *h, int n_groups, const int64_t 
     p->n_heavy.resize(n_groups);
     p->err_bound.resize(n_groups);
     p->sum_abs.resize(n_groups);
+    p->err_dd.resize(n_groups);
+    p->err_dk.resize(n_groups);
     p->shape_nzw.resize(n_groups);
     p->heavy_chunk.assign(n_groups, 0);
     p->light_chunk.assign(n_groups, 0);
@@ -380,6 +394,14 @@ extern "C" int mb_plan_set_skip(mb_plan *p, double skip_frac) {
     replan_tiers(p);
     MB_TRY(device_guard(p->table->device));
     return upload(p);
+}
+
+extern "C" int mb_plan_group_bounds(const mb_plan *p, int g, double *val, double *dd, double *dk) {
+    MB_CHECK_ARG(p && g >= 0 && g < p->n_groups, "mb_plan_group_bounds: bad plan/group");
+    if (val) *val = p->err_bound[g];
+    if (dd) *dd = p->err_dd[g];
+    if (dk) *dk = p->err_dk[g];
+    return MB_OK;
 }
 
 extern "C" int mb_plan_group_zeros(const mb_plan *p, int g, int64_t *n_eval) {

@@ -190,11 +190,12 @@ class Plan:
 
     def group_info(self, g: int):
         nT, nh, eb, sa = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
-        ne = C.c_int64()
+        ne, bd, bk = C.c_int64(), C.c_double(), C.c_double()
         check(_lib.lib().mb_plan_group_info(self.handle, g, C.byref(nT), C.byref(nh), C.byref(eb), C.byref(sa)))
         check(_lib.lib().mb_plan_group_zeros(self.handle, g, C.byref(ne)))
+        check(_lib.lib().mb_plan_group_bounds(self.handle, g, None, C.byref(bd), C.byref(bk)))
         return {"n_T": nT.value, "n_eval": ne.value, "n_heavy": nh.value, "err_bound": eb.value,
-                "sum_abs": sa.value}
+                "err_bound_dd": bd.value, "err_bound_dk": bk.value, "sum_abs": sa.value}
 
     def run(self, cands):
         """Host arrays in, host arrays out (graph replay through pinned staging)."""

@@ -142,3 +142,20 @@ def test_plan_ragged_and_empty_groups(table, small_table):
                 assert np.all(val[off:off + c] == 0) and np.all(pv == 0)
             assert np.max(np.abs(val[off:off + c] - pv)) <= gi["err_bound"] + 1e-15
             off += c
+
+
+@pytest.mark.parametrize("k,skip", [(3e-9, 0.0), (1e-9, 0.0), (1e-8, 0.25)])
+def test_derivative_bounds(table, small_table, oracle, k, skip):
+    """K2, dK2/ddelta and dK2/dk each within their plan's a-priori bound of the oracle."""
+    cd = synth.make_candidates(64, seed=13)
+    cd.delta[:] = np.random.default_rng(14).uniform(-1e-4, 1e-4, 64)
+    ohi, _ = oracle.k2(cd, small_table, k, small_table.n)
+    with k2.Plan(table, [64], [k], [math.inf], tol=TOL) as plan:
+        plan.set_skip(skip)
+        val, dd, dk = plan.run(cd)
+        gi = plan.group_info(0)
+    assert gi["err_bound"] <= TOL
+    for got, q, key in ((val, 0, "err_bound"), (dd, 1, "err_bound_dd"), (dk, 2, "err_bound_dk")):
+        assert np.max(np.abs(got - ohi[:, q])) <= gi[key], key
+    # the derivative bounds scale with gamma and gamma^2 of the zeros that matter
+    assert gi["err_bound"] < gi["err_bound_dd"] < gi["err_bound_dk"]
