@@ -82,12 +82,22 @@ def autotune(plan: k2.Plan, reps: int = 3, use_cache: bool = True, space=SPACE) 
                     "cached": True, "key": key}
     timings = {}
     best = None
-    for cfg in space:
-        plan.configure(*cfg)
-        ms = plan.time(reps)
-        timings[f"{cfg[0]}/{cfg[1]}/{cfg[2]}"] = ms
-        if best is None or ms < best[1]:
-            best = (cfg, ms)
+    if space == SPACE:                          # the library's own search over the same space
+        import ctypes as C
+        from ._lib import check, lib
+        cpt, shift, scale, ms = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+        t = (C.c_double * len(SPACE))()
+        check(lib().mb_plan_autotune(plan.handle, int(reps), C.byref(cpt), C.byref(shift), C.byref(scale),
+                                     C.byref(ms), t))
+        timings = {f"{c}/{sh}/{sc}": t[i] for i, (c, sh, sc) in enumerate(SPACE)}
+        best = ((cpt.value, shift.value, scale.value), ms.value)
+    else:
+        for cfg in space:
+            plan.configure(*cfg)
+            ms = plan.time(reps)
+            timings[f"{cfg[0]}/{cfg[1]}/{cfg[2]}"] = ms
+            if best is None or ms < best[1]:
+                best = (cfg, ms)
     plan.configure(*best[0])
     if use_cache:
         with _lock:

@@ -465,6 +465,40 @@ extern "C" int mb_plan_time(mb_plan *p, int reps, double *ms) {
     return MB_OK;
 }
 
+// The autotuner's search: every (light_cpt, nzw_shift, chunk_scale) in {2, 3, 4} x {0, 1} x
+// {0.5, 1, 2} (in that nesting order) timed by mb_plan_time(reps); the fastest is applied.
+extern "C" int mb_plan_autotune(mb_plan *p, int reps, int *light_cpt, int *nzw_shift, double *chunk_scale,
+                                double *best_ms, double *timings) {
+    MB_CHECK_ARG(p && reps >= 1 && reps <= 1000, "mb_plan_autotune: bad argument");
+    static const int cpts[3] = {2, 3, 4};
+    static const int shifts[2] = {0, 1};
+    static const double scales[3] = {0.5, 1.0, 2.0};
+    int bc = 4, bs = 0;
+    double bsc = 1.0, bms = INFINITY;
+    int i = 0;
+    for (int c : cpts)
+        for (int sh : shifts)
+            for (double sc : scales) {
+                MB_TRY(mb_plan_configure(p, c, sh, sc));
+                double ms = 0;
+                MB_TRY(mb_plan_time(p, reps, &ms));
+                if (timings) timings[i] = ms;
+                ++i;
+                if (ms < bms) {
+                    bms = ms;
+                    bc = c;
+                    bs = sh;
+                    bsc = sc;
+                }
+            }
+    MB_TRY(mb_plan_configure(p, bc, bs, bsc));
+    if (light_cpt) *light_cpt = bc;
+    if (nzw_shift) *nzw_shift = bs;
+    if (chunk_scale) *chunk_scale = bsc;
+    if (best_ms) *best_ms = bms;
+    return MB_OK;
+}
+
 extern "C" int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, int *n_items) {
     MB_CHECK_ARG(p, "mb_plan_info: null plan");
     if (P) *P = p->P;
