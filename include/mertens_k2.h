@@ -58,6 +58,7 @@ int mb_abi_version(void);
  * non-finite c, G integer part >= 2^32, or |gamma - 2pi G| > 4 ulp(gamma). */
 int mb_table_create(const uint64_t *G3, const double *c_re, const double *c_im, const double *gamma,
                     int64_t n, int device, mb_table **out);
+/* Fails with MB_ERR_STATE while plans created on the table are alive (destroy them first). */
 int mb_table_destroy(mb_table *t);
 int mb_table_size(const mb_table *t, int64_t *n_out);
 /* Number of zeros with gamma < T. */

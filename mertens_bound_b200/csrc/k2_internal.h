@@ -71,6 +71,7 @@ struct Table {
     // grow-only scratch owned by the table: `io` stages candidates and results of host-pointer
     // calls, `work` holds per-chunk partial sums.  Calls on one table must not overlap on the GPU.
     DevBuf io, work;
+    int n_plans = 0;                  // live plans on this table (it cannot be destroyed under them)
 
     int64_t count_below(double T) const;
 };

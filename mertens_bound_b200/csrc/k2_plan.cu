@@ -328,6 +328,7 @@ extern "C" int mb_plan_create_weighted(mb_table *h, int n_groups, const int64_t 
         delete p;
         return st;
     }
+    ++t.n_plans;
     *out = p;
     return MB_OK;
 }
@@ -342,6 +343,7 @@ extern "C" int mb_plan_destroy(mb_plan *p) {
     device_guard(p->table->device);
     free_io(p);
     free_dev(p);
+    --p->table->n_plans;
     delete p;
     return MB_OK;
 }

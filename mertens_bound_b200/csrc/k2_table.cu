@@ -193,6 +193,10 @@ extern "C" int mb_table_create(const uint64_t *G3, const double *c_re, const dou
 
 extern "C" int mb_table_destroy(mb_table *h) {
     if (!h) return MB_OK;
+    if (h->t.n_plans > 0) {
+        set_error("mb_table_destroy: %d plan(s) still use this table; destroy them first", h->t.n_plans);
+        return MB_ERR_STATE;
+    }
     device_guard(h->t.device);
     free_table(h->t);
     delete h;

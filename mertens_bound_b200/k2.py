@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes as C
 import hashlib
 import math
+import weakref
 
 import numpy as np
 
@@ -80,8 +81,12 @@ class ZeroTable:
         return out.value
 
     def close(self):
+        """Free the device table, closing first any plan made on it that is still open (the
+        library refuses to free a table under live plans)."""
         if getattr(self, "_h", None) is not None:
-            _lib.lib().mb_table_destroy(self._h)
+            for plan in list(self.__dict__.get("_plans", ())):
+                plan.close()
+            check(_lib.lib().mb_table_destroy(self._h))
             self._h = None
 
     def __enter__(self):
@@ -152,6 +157,7 @@ class Plan:
                                                      ptr(Ts), ptr(weights), float(tol), C.byref(h)))
         self._h = h
         self.table = table
+        table.__dict__.setdefault("_plans", weakref.WeakSet()).add(self)
         self.counts, self.ks, self.Ts, self.tol = counts, ks, Ts, tol
         self.P = int(counts.sum())
 

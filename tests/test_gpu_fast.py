@@ -159,3 +159,16 @@ def test_derivative_bounds(table, small_table, oracle, k, skip):
         assert np.max(np.abs(got - ohi[:, q])) <= gi[key], key
     # the derivative bounds scale with gamma and gamma^2 of the zeros that matter
     assert gi["err_bound"] < gi["err_bound_dd"] < gi["err_bound_dk"]
+
+
+def test_table_outlives_its_plans(gpu, small_table):
+    """The library refuses to free a table under a live plan; the Python table closes its plans."""
+    from mertens_bound_b200._lib import lib
+    t = k2.ZeroTable.from_data(small_table.truncate(2000))
+    plan = k2.Plan(t, [8], [3e-9], [math.inf])
+    assert lib().mb_table_destroy(t.handle) == -5          # MB_ERR_STATE
+    assert "plan" in lib().mb_last_error().decode()
+    plan.run(synth.make_candidates(8, seed=1))             # the table is intact
+    t.close()
+    with pytest.raises(ValueError):
+        plan.handle
