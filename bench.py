@@ -513,6 +513,37 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
         except Exception as e:                                       # the baseline is optional
             ds["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
     out["driver_scoring"] = ds
+
+    # the enumerators' two GPU steps and the peak re-optimisation, each on the 600,000-zero table:
+    #   enumerator_screen  2^20 random leaves through the GPU screen (64/128/256 zeros, 7 offsets)
+    #   hit_polish         256 hits through the five ZeroData::polish stages
+    #   polish_scan        search/polish.py's default grid (half 0.25, step 2e-5: 25,001 points) over
+    #                      the zeros below 74,000 at the Peak2 point
+    from mertens_bound_b200 import hit_polish, polish
+    with k2.ZeroTable.from_data(d600, device=dev.index) as t6:
+        cl = synth.make_candidates(1 << 20, seed=7)
+        pts = np.stack([cl.v_int, cl.v_frac], axis=1)
+        hit_polish.screen_leaves(t6, pts[:4096])
+        t0 = time.perf_counter()
+        r = hit_polish.screen_leaves(t6, pts, max_hits=1 << 20)
+        sc_s = time.perf_counter() - t0
+        out["enumerator_screen"] = {"leaves": len(pts), "seconds": sc_s, "leaves_per_s": len(pts) / sc_s,
+                                    "hits": int(len(r.hits)), "stages": "64/128/256 zeros, 0.78/0.855/0.892",
+                                    "note": "host-pointer call: includes the H2D of 16 MB of leaves"}
+        hits = pts[:256]
+        hit_polish.polish_hits(t6, hits[:8])
+        t0 = time.perf_counter()
+        hr = hit_polish.polish_hits(t6, hits, thresholds=(None, None, None))
+        hp_s = time.perf_counter() - t0
+        out["hit_polish"] = {"hits": 256, "zeros": d600.n, "seconds": hp_s, "hits_per_s": 256 / hp_s,
+                             "stages_run": int(hr.stage.max()) + 1, "thresholds": "none (every hit runs all stages)"}
+        n74 = t6.count_below(polish.POLISH_T)
+        polish.scan(t6, synth.PEAK2_STR, 0.001, 2e-5)
+        t0 = time.perf_counter()
+        best, y_best, m_best = polish.scan(t6, synth.PEAK2_STR, 0.25, 2e-5)
+        ps_s = time.perf_counter() - t0
+        out["polish_scan"] = {"points": 25001, "zeros": n74, "seconds": ps_s,
+                              "point_zero_terms_per_s": 25001 * n74 / ps_s, "best_abs_h": abs(best)}
     return out
 
 
