@@ -135,8 +135,8 @@ void replan_tiers(mb_plan *p) {
 }
 
 // Work items.  Heavy items (FP64 tier) use HEAVY_CPT candidates per thread and are pulled by
-// the persistent heavy kernel (one CTA per SM); light items use the plan's light_cpt and run
-// one CTA each.  Chunk sizes aim at ~8 heavy items per heavy CTA and ~24 light items per SM.
+// the persistent heavy kernel (two CTAs per SM); light items use the plan's light_cpt and run
+// one CTA each.  Chunk sizes aim at ~4 heavy items and ~18 light items per SM.
 int build_items(mb_plan *p, int sms) {
     p->groups.clear();
     p->items.clear();
@@ -151,7 +151,7 @@ int build_items(mb_plan *p, int sms) {
         Wh += (double)p->counts[g] * std::max<int64_t>(0, he(g) - hb(g));
         Wl += (double)p->counts[g] * std::max<int64_t>(0, le(g) - lb(g));
     }
-    // ~4 items per heavy CTA (one per SM) and ~6 waves of light CTAs (about 3 per SM)
+    // ~4 heavy items per SM (two per heavy CTA) and ~18 light items per SM (several waves)
     const double target_h = std::max(p->chunk_scale * Wh / (4.0 * sms), 1.0);
     const double target_l = std::max(p->chunk_scale * Wl / (18.0 * sms), 1.0);
     std::vector<FastItem> heavy, light;
