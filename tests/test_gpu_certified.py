@@ -70,3 +70,22 @@ def test_certified_full_peak2(gpu, oracle):
     v = ohi[0, 0] + olo[0, 0]
     assert lo[0] <= v <= hi[0]
     assert hi[0] - lo[0] < 1e-11
+
+
+def test_certified_maximum_batch(table, small_table, oracle):
+    """The largest batch one call takes (65,535 points) encloses the plain FP64 values (a
+    sample checked against the binary128 oracle); one more point is rejected."""
+    from mertens_bound_b200._lib import K2Error
+    cd = synth.make_candidates(65_535, seed=54)
+    T = 2000.0
+    lo, hi, _ = k2.k2_certified(table, cd, 3e-9, T)
+    pv, _, _ = k2.k2_plain(table, cd, 3e-9, T)
+    width = hi - lo
+    assert np.max(width) < 1e-12
+    assert np.all(lo - width <= pv) and np.all(pv <= hi + width)     # plain is within ~1e-15
+    idx = np.arange(0, 65_535, 4_096)
+    ohi, olo = oracle.k2(cd.subset(idx), small_table, 3e-9, small_table.count_below(T))
+    v = ohi[:, 0] + olo[:, 0]
+    assert np.all(lo[idx] <= v) and np.all(v <= hi[idx])
+    with pytest.raises(K2Error, match="MB_ERR_ARG"):
+        k2.k2_certified(table, synth.make_candidates(65_536, seed=55), 3e-9, T)
