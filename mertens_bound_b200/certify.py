@@ -294,18 +294,36 @@ def certify(data, v_str: str = V_STR, k_str: str = K_STR, T0_str: str = T0_STR, 
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description="Certified K2 on the GPU (certify_K2.py contract)")
+    # certify_K2.py's command line: [workers] --v --k --out --cache-only (:137-142)
+    ap.add_argument("workers", nargs="?", type=int, default=None,
+                    help="accepted for certify_K2.py's command line; the GPU kernel needs no worker pool")
     ap.add_argument("--v", default=V_STR)
     ap.add_argument("--k", default=K_STR)
     ap.add_argument("--T0", default=T0_STR)
     ap.add_argument("--table", default=None, help="zero-cache .txt (default: synthetic zeros below T0)")
+    ap.add_argument("--cache-dir", default=None,
+                    help="directory of zero-cache files ({n0:08d}_{num}_{dps}.txt, read in name order)")
+    ap.add_argument("--cache-only", action="store_true",
+                    help="certify_K2.py's zero generation step: not part of this evaluator")
     ap.add_argument("--batch", type=int, default=0, help="certify in batches with a key-checked cache")
     ap.add_argument("--out", default="k2_certificate.json")
     a = ap.parse_args(argv)
+    if a.cache_only:
+        print("FAIL: --cache-only generates zeros (acb.zeta_zeros); this evaluator only reads zero caches",
+              file=sys.stderr)
+        return 2
     try:
         term_rad = None
-        if a.table:
+        files = None
+        if a.cache_dir:
+            import glob
+            files = sorted(glob.glob(os.path.join(a.cache_dir, "*.txt")))
+            require(files, f"no zero-cache files in {a.cache_dir}")
+        elif a.table:
+            files = [a.table]
+        if files:
             from . import formats
-            data, radii = formats.read_zero_cache(a.table)
+            data, radii = formats.read_zero_cache(files)
             term_rad = formats.term_radius(radii, data, float(Fraction(a.v)))
         else:
             # synthetic zeros a little beyond T0, so the gap around T0 can be certified

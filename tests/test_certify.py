@@ -91,3 +91,26 @@ def test_cli_exit_codes(gpu, tmp_path):
     assert certify.main(["--T0", "2000", "--k", "3e-9", "--out", out]) == 0
     assert json.load(open(out))["N_T0"] > 0
     assert certify.main(["--T0", "10", "--out", out]) == 1             # no zeros below T0
+
+
+def test_cli_cache_only_refused():
+    """certify_K2.py's zero-generation mode is outside the evaluator: a clear refusal, exit 2."""
+    assert certify.main(["24", "--cache-only"]) == 2
+
+
+@pytest.mark.gpu
+def test_cli_reads_cache_dir(gpu, tmp_path):
+    """certify_K2.py's command line ([workers] --v --k --out) over a zero_cache/ directory."""
+    from mertens_bound_b200 import formats, synth
+    data = synth.make_table_below(1500.0, seed=3)
+    half = data.n // 2
+    d = tmp_path / "zero_cache"
+    d.mkdir()
+    formats.write_zero_cache(str(d / f"{1:08d}_{half}_45.txt"), data.truncate(half))
+    rest = synth.ZeroTableData(data.G3[half:].copy(), data.gamma[half:].copy(), data.c_re[half:].copy(),
+                               data.c_im[half:].copy(), data.seed)
+    formats.write_zero_cache(str(d / f"{half + 1:08d}_{data.n - half}_45.txt"), rest)
+    out = str(tmp_path / "c.json")
+    assert certify.main(["24", "--k", "3e-9", "--T0", "1000", "--cache-dir", str(d), "--out", out]) == 0
+    cert = json.load(open(out))
+    assert cert["N_T0"] == data.count_below(1000.0)
