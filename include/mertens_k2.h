@@ -146,7 +146,7 @@ int mb_plan_destroy(mb_plan *p);
 /* Tail skip: give the share skip_frac (0 .. 0.25) of tol to not evaluating, per group, the zeros
  * beyond the point where the remaining sum of 2|c| w is <= skip_frac * tol (the Gaussian makes
  * most zeros below a large T negligible at tol = 1e-10: ~76% of them at T = 3e5, k = 3e-9).
- * The light tier keeps (1/2 - skip_frac) tol; the group bound includes the skipped sum; the
+ * The light tier fits in what remains of tol; the group bound includes the skipped sum; the
  * derivative outputs omit the same zeros.  0 (the default) evaluates every zero below T, as the
  * reference does.  No reference counterpart (it sums every zero below its cutoff). */
 int mb_plan_set_skip(mb_plan *p, double skip_frac);

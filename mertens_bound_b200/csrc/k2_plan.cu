@@ -79,7 +79,8 @@ int default_nzw(int64_t P, int cpt) {
 // group's weight vector):
 //   n_eval: the smallest n with sum_{n <= j < n_use} a_j <= skip_frac * tol -- those zeros are
 //           not evaluated (skip_frac = 0: every zero below T is evaluated);
-//   n_h:    the smallest n_h with EPS_LIGHT * sum_{n_h <= j < n_eval} a_j <= (1/2 - skip_frac) tol.
+//   n_h:    the smallest n_h that keeps the whole bound (skipped sum + EPS_LIGHT * light sum +
+//           EPS_HEAVY * heavy sum + FP64 roundings) within 0.99 tol.
 // Returns the a-priori bound of |K2 error| (skipped sum + tier errors + FP64 roundings).
 void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, double tol, double skip_frac,
                 int64_t &n_eval, int64_t &n_h, double &bound, double &sabs, double &bound_dd, double &bound_dk) {
@@ -98,19 +99,22 @@ void plan_tiers(const Table &t, int64_t n_use, double k, const double *wts, doub
             skipped += a[j];
             n_eval = j;
         }
-    const double budget = (0.5 - skip_frac) * tol;
+    // The light tier takes zeros from the top while the whole bound stays within 0.99 tol
+    // (the heavy tier's and the roundings' shares are tiny, so nearly all of the rest of tol).
+    // FP64 accumulation and reduction of the heavy sum and of the light partials: at most
+    // ~(terms per thread + chunks) roundings of 2^-53 relative; 1e-13 relative is a safe cover.
+    const double evaluated = total - skipped;
+    const double fixed = skipped + 1e-13 * evaluated;
     double tail = 0;
     n_h = n_eval;
     for (int64_t j = n_eval - 1; j >= 0; --j) {
-        if ((tail + a[j]) * EPS_LIGHT > budget) break;
-        tail += a[j];
+        const double t2 = tail + a[j];
+        if (fixed + EPS_LIGHT * t2 + EPS_HEAVY * (evaluated - t2) > 0.99 * tol) break;
+        tail = t2;
         n_h = j;
     }
-    const double evaluated = total - skipped;
     double heavy = evaluated - tail;
-    // FP64 accumulation and reduction of the heavy sum and of the light partials: at most
-    // ~(terms per thread + chunks) roundings of 2^-53 relative; 1e-13 relative is a safe cover.
-    bound = skipped + EPS_LIGHT * tail + EPS_HEAVY * heavy + 1e-13 * evaluated;
+    bound = fixed + EPS_LIGHT * tail + EPS_HEAVY * heavy;
     sabs = total;
     // the derivative terms are the value terms with amplitudes a gamma and a gamma^2 (computed
     // the same way in each tier), so the same per-unit errors apply to those amplitude sums
@@ -386,7 +390,7 @@ extern "C" int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, doubl
 
 // Give the share skip_frac (0 .. 1/4) of tol to not evaluating each group's negligible tail: the
 // zeros beyond the point where the remaining sum of 2|c| w is <= skip_frac tol are skipped, and
-// the light tier keeps (1/2 - skip_frac) tol.  The bound of mb_plan_group_info includes the
+// the light tier fits in what remains of tol.  The bound of mb_plan_group_info includes the
 // skipped sum.  (The derivative outputs then omit sum 2|c| w gamma and 2|c| w gamma^2 over the
 // same zeros.)  0 restores the evaluation of every zero below T.
 extern "C" int mb_plan_set_skip(mb_plan *p, double skip_frac) {
