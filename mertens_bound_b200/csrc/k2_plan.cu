@@ -41,7 +41,11 @@ struct mb_plan {
     void *h_pinned = nullptr;
     cudaGraphExec_t graph = nullptr;
     DevBuf newton_buf;             // Newton polish: starting point, its gradients, stop flags
-    ~mb_plan() { newton_buf.release(); }
+    DevBuf flush_buf;              // mb_plan_time: written between timed runs to empty the L2
+    ~mb_plan() {
+        newton_buf.release();
+        flush_buf.release();
+    }
 };
 
 namespace {
@@ -428,7 +432,8 @@ extern "C" int mb_plan_set_zero_range(mb_plan *p, int64_t j0, int64_t j1) {
 }
 
 // Median device time (ms) of `reps` runs of the plan on synthetic candidates (the values do not
-// change the work), after one warm-up run.  Used by the autotuner.
+// change the work), after one warm-up run, each run after a 192 MB write that empties the L2.
+// Used by the autotuner.
 extern "C" int mb_plan_time(mb_plan *p, int reps, double *ms) {
     MB_CHECK_ARG(p && ms && reps >= 1 && reps <= 1000, "mb_plan_time: bad argument");
     MB_TRY(device_guard(p->table->device));
@@ -448,12 +453,20 @@ extern "C" int mb_plan_time(mb_plan *p, int reps, double *ms) {
     MB_CUDA(cudaMemcpyAsync(p->d_vi, v.data(), P * 8, cudaMemcpyHostToDevice, s));
     MB_CUDA(cudaMemcpyAsync(p->d_vf, v.data() + P, P * 8, cudaMemcpyHostToDevice, s));
     MB_CUDA(cudaMemsetAsync(p->d_delta, 0, P * 8, s));
+    // each timed run starts from an empty L2 (the 126 MB L2 would otherwise keep the table)
+    const size_t flush_bytes = (size_t)192 << 20;
+    MB_TRY(p->flush_buf.ensure(flush_bytes));
     cudaEvent_t e0, e1;
     MB_CUDA(cudaEventCreate(&e0));
     MB_CUDA(cudaEventCreate(&e1));
     std::vector<float> t;
     int st = plan_run_dev(p, p->d_vi, p->d_vf, p->d_delta, p->d_out, p->d_out + P, p->d_out + 2 * P, s);
     for (int r = 0; r < reps && st == MB_OK; ++r) {
+        if (cudaMemsetAsync(p->flush_buf.p, r & 0xff, flush_bytes, s) != cudaSuccess) {
+            st = MB_ERR_CUDA;
+            set_error("mb_plan_time: L2 flush failed");
+            break;
+        }
         cudaEventRecord(e0, s);
         st = plan_run_dev(p, p->d_vi, p->d_vf, p->d_delta, p->d_out, p->d_out + P, p->d_out + 2 * P, s);
         cudaEventRecord(e1, s);
