@@ -176,12 +176,12 @@ int build_items(mb_plan *p, int sms) {
         const int64_t CTl = (int64_t)(8 / nzw) * 32 * p->light_cpt;
         int64_t hz = p->heavy_chunk[g], lz = p->light_chunk[g];
         // chunk = target terms / tile candidates, rounded to whole tiles (at least 1 heavy tile of
-        // 128 zeros, 4 light tiles of 256: finer heavy items balance the persistent kernel better,
-        // measured)
+        // 128 zeros and 8 light tiles of 256: finer heavy items balance the persistent kernel,
+        // coarser light items cost less per term -- both measured)
         if (hz <= 0)
             hz = std::max<int64_t>(128, ((int64_t)(target_h / std::min<int64_t>(CTh, std::max<int64_t>(gr.nc, 1))) + 64) / 128 * 128);
         if (lz <= 0)
-            lz = std::max<int64_t>(1024, ((int64_t)(target_l / std::min<int64_t>(CTl, std::max<int64_t>(gr.nc, 1))) + 128) / 256 * 256);
+            lz = std::max<int64_t>(2048, ((int64_t)(target_l / std::min<int64_t>(CTl, std::max<int64_t>(gr.nc, 1))) + 128) / 256 * 256);
         int ch = 0;
         auto emit = [&](int64_t z0, int64_t z1, int tier, int64_t CT, int cpt, std::vector<FastItem> &dst) {
             for (int64_t ct = 0; ct * CT < gr.nc; ++ct) {
