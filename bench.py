@@ -42,13 +42,14 @@ UNIT = "zero-terms/s"
 T0, K_GAUSS, P_PER_GPU, TOL = 3e5, 3e-9, 4096, 1e-10
 WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 candidates v~3.5e18 "
             "per GPU, k=3e-9, K2 + dK2/ddelta + dK2/dk per candidate, a-priori |err| <= 1e-10")
-# Warp instructions per warp of zero-terms (= thread instructions per zero-term) of the light-tier
-# kernel (the dominant kernel) for each candidates-per-thread setting, from the ncu capture of
-# `bench.py --profile-case search` summarised in profiles/k2_light_kernel_search_scoring.md.
-LIGHT_INST_PER_TERM = {2: 23.43, 3: 25.67, 4: 20.07}
-# DRAM bytes per light launch on this workload (same captures): reads of the zero tiles and
-# candidates; writes ~0.
-LIGHT_DRAM_BYTES = {2: 16419840, 3: 16779520, 4: 16581120}
+# Warp instructions per warp of zero-terms (= thread instructions per zero-term) of the two
+# tier kernels -- the light tier for each candidates-per-thread setting -- and their DRAM bytes
+# per launch on this workload, from the ncu capture of `bench.py --profile-case search`
+# summarised in profiles/k2_light_kernel_search_scoring.md.
+LIGHT_INST_PER_TERM = {2: 23.40, 3: 25.62, 4: 20.03}
+HEAVY_INST_PER_TERM = 53.94
+LIGHT_DRAM_BYTES = {2: 16487680, 3: 16466176, 4: 16446464}
+HEAVY_DRAM_BYTES = 2775040
 REF_SAMPLE_CANDS = 64
 
 
@@ -273,7 +274,12 @@ def run_ours(args):
     heavy_ms = statistics.median(timed(lambda: fast(1), 5, 1))
     ht, lt = C_double_pair(L.mb_plan_tier_terms, plan.handle)
     peak = C_double(L.mb_calibrate_issue, local)
-    inst_per_term = LIGHT_INST_PER_TERM[tuned["config"][0]]
+    # the timed step runs the two tier kernels concurrently (plus a small reduction): the roof is
+    # the instruction issue of the whole step; the light kernel alone is reported beside it
+    cpt = tuned["config"][0]
+    inst_per_term = LIGHT_INST_PER_TERM[cpt]
+    step_inst = inst_per_term * lt + HEAVY_INST_PER_TERM * ht
+    step_achieved = step_inst / (ms_per_step * 1e-3)
     light_achieved = inst_per_term * lt / (light_ms * 1e-3)
 
     # end to end through the host-pointer API (pinned H2D, graph, D2H), every step
@@ -316,14 +322,18 @@ def run_ours(args):
         "max_abs_diff_vs_plain": {"val": float(diff[0]), "dd": float(diff[1]), "dk": float(diff[2])},
         "err_vs_certified": err_vs_cert,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * P, "d2h_bytes_per_step": 3 * 8 * P},
-        "roofline": {"bound": "issue", "kernel": "k2_light_kernel", "achieved": light_achieved / 1e12,
-                     "peak": peak / 1e12, "unit": "T thread-inst/s", "frac": light_achieved / peak,
-                     "traffic": LIGHT_DRAM_BYTES[tuned["config"][0]], "traffic_unit": "bytes/launch",
-                     "per_term_inst": inst_per_term, "light_ms": light_ms,
-                     "heavy_ms": heavy_ms, "light_terms": lt, "heavy_terms": ht,
+        "roofline": {"bound": "issue", "kernel": "k2_light_kernel + k2_heavy_kernel (concurrent, one step)",
+                     "achieved": step_achieved / 1e12, "peak": peak / 1e12, "unit": "T thread-inst/s",
+                     "frac": step_achieved / peak,
+                     "traffic": LIGHT_DRAM_BYTES[cpt] + HEAVY_DRAM_BYTES, "traffic_unit": "bytes/step",
+                     "inst_per_term": {"light": inst_per_term, "heavy": HEAVY_INST_PER_TERM},
+                     "light_terms": lt, "heavy_terms": ht,
+                     "light_alone": {"ms": light_ms, "achieved": light_achieved / 1e12,
+                                     "frac": light_achieved / peak},
+                     "heavy_alone_ms": heavy_ms,
                      "peak_source": "measured live: FFMA issue rate (mb_calibrate_issue); MEASURED_PEAKS.json "
-                                    "has only HBM and bf16-tensor peaks, neither binds this kernel",
-                     "hbm": hbm_line(LIGHT_DRAM_BYTES[tuned["config"][0]], light_ms)},
+                                    "has only HBM and bf16-tensor peaks, neither binds these kernels",
+                     "hbm": hbm_line(LIGHT_DRAM_BYTES[cpt] + HEAVY_DRAM_BYTES, ms_per_step)},
         "clocks": clocks,
         "gpu_launches": 3 * args.steps,
         "tail_skip": tail_skip,
