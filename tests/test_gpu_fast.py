@@ -172,3 +172,32 @@ def test_table_outlives_its_plans(gpu, small_table):
     t.close()
     with pytest.raises(ValueError):
         plan.handle
+
+
+def test_shards_with_skip_and_weights(gpu, oracle):
+    """Zero-range shards of a plan with a tail skip and a mix of weight vectors add up to the
+    unsharded run, and each group stays within its bound of the oracle."""
+    from mertens_bound_b200 import distributed, score
+    from mertens_bound_b200._lib import check, lib
+    data = synth.make_table(40_000, seed=8)
+    cd = synth.make_candidates(96, seed=81)
+    W = score.reference_weights(data.gamma)
+    with k2.ZeroTable.from_data(data) as t:
+        slots = [t.add_weights(W["jp"]), -1, t.add_weights(W["g15"])]
+        with k2.Plan(t, [32, 32, 32], [0.0, 1e-8, 0.0], [math.inf, math.inf, 20000.0], tol=TOL,
+                     weights=slots) as plan:
+            plan.set_skip(0.25)
+            full = np.stack(plan.run(cd), axis=1)
+            bounds = [plan.group_info(g) for g in range(3)]
+            parts = []
+            for r in range(4):
+                j0, j1 = distributed.shard_range(t.n, 4, r)
+                check(lib().mb_plan_set_zero_range(plan.handle, j0, j1))
+                parts.append(np.stack(plan.run(cd), axis=1))
+    tot = sum(parts)
+    for g, (w, k, T) in enumerate(((W["jp"], 0.0, math.inf), (None, 1e-8, math.inf), (W["g15"], 0.0, 20000.0))):
+        sl = slice(32 * g, 32 * g + 32)
+        n = data.count_below(T)
+        ohi, _ = oracle.k2(cd.subset(np.arange(32 * g, 32 * g + 32)), data, k, n, weights=w)
+        assert np.max(np.abs(full[sl, 0] - ohi[:, 0])) <= bounds[g]["err_bound"]
+        assert np.max(np.abs(tot[sl, 0] - full[sl, 0])) <= 2 * bounds[g]["err_bound"]
