@@ -529,7 +529,7 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
     #   hit_polish         256 hits through the five ZeroData::polish stages
     #   polish_scan        search/polish.py's default grid (half 0.25, step 2e-5: 25,001 points) over
     #                      the zeros below 74,000 at the Peak2 point
-    from mertens_bound_b200 import hit_polish, polish
+    from mertens_bound_b200 import hit_polish, path1, polish
     with k2.ZeroTable.from_data(d600, device=dev.index) as t6:
         cl = synth.make_candidates(1 << 20, seed=7)
         pts = np.stack([cl.v_int, cl.v_frac], axis=1)
@@ -554,6 +554,39 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
         ps_s = time.perf_counter() - t0
         out["polish_scan"] = {"points": 25001, "zeros": n74, "seconds": ps_s,
                               "point_zero_terms_per_s": 25001 * n74 / ps_s, "best_abs_h": abs(best)}
+
+    # taylor_polish: search/path1_kernel_opt.py's fast_polish_batch_blas contract (degree-16
+    # moments, 121-point grid, exact Newton on the top 25) for 1,024 candidates over its 100,000
+    # zeros with the JP weight, matrix-free; beside it the reference algorithm (numpy/BLAS
+    # restatement) on A/B rows from the reference's compiled compute_peak_AB
+    d100 = big.truncate(100_000)
+    c7 = synth.make_candidates(1024, seed=8)
+    w_jp = score.reference_weights(d100.gamma)["jp"]
+    with k2.ZeroTable.from_data(d100, device=dev.index) as t7:
+        slot = t7.add_weights(w_jp)
+        path1.fast_polish_exact(t7, c7.subset(np.arange(64)), slot)
+        t0 = time.perf_counter()
+        path1.fast_polish_exact(t7, c7, slot)
+        tp_s = time.perf_counter() - t0
+    tp = {"candidates": 1024, "zeros": 100_000, "seconds": tp_s, "candidates_per_s": 1024 / tp_s,
+          "top": 25, "grid": "121 points on [-3e-5, 3e-5]"}
+    if cpu_baseline:
+        try:
+            from oracle import polish_ref
+            from oracle.oracle import RefLib, reference_candidates, reference_format
+            if RefLib.available():
+                sub = c7.subset(np.arange(128))
+                A, B = RefLib().peak_AB(reference_candidates(sub), reference_format(d100, exact_psi=False))
+                t0 = time.perf_counter()
+                polish_ref.fast_polish_batch(A, B, d100.gamma, w_jp)
+                cs = time.perf_counter() - t0
+                tp["cpu_baseline"] = {"kind": "port", "cores": os.cpu_count(), "candidates": 128, "seconds": cs,
+                                      "candidates_per_s": 128 / cs,
+                                      "sample": "numpy/BLAS restatement of fast_polish_batch_blas on A/B rows "
+                                                "(A/B build not timed)"}
+        except Exception as e:
+            tp["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    out["taylor_polish"] = tp
     return out
 
 
