@@ -2,8 +2,9 @@
 //
 // Each group (k, T, a range of candidates) splits its zeros [0, n_T) at a boundary n_h chosen
 // from an a-priori error bound (host, k2_plan.cu):
-//   heavy tier  j <  n_h : 64-bit phase (3 IMAD.lo + 8 DFMA, error ~2^-48 turn), quarter-turn
-//                          FP64 polynomials, FP64 accumulation.          -> k2_heavy_kernel
+//   heavy tier  j <  n_h : 64-bit phase (3 IMAD.lo + 4 DFMA + 4 FFMA, error ~2^-48 turn), sin/cos
+//                          from a 1024-entry table rotated by short FP64 polynomials, FP64
+//                          accumulation.                                  -> k2_heavy_kernel
 //   light tier  j >= n_h : 32-bit phase (3 IMAD.lo + 4 DFMA in two chains), MUFU sin/cos of
 //                          the reduced phase, FP32 accumulation flushed every LIGHT_FLUSH terms
 //                          into FP64 partials.                           -> k2_light_kernel
@@ -37,11 +38,11 @@ struct __align__(16) ZLight {   // 64 B
     float a, b, d, pad;          // a = 2|c|w, b = -a gamma, d = -a gamma^2
 };
 
-struct __align__(16) ZHeavy {   // 112 B
-    uint32_t b0, b1, gi, pad;
+struct __align__(16) ZHeavy {   // 96 B
+    uint32_t b0, b1, gi, psi_hi; // psi_hi = top 32 bits of arg(c)/2pi 2^64
     double b0s, c1s, gis, b1s;   // limb 2^-64
-    double c0t, c1t, b0t, b1t;   // limb 2^-96
-    double psi;                  // arg(c)/2pi in turns
+    float c0f, c1f, b0f, b1f;    // limb 2^-96 (FP32: these products need 2^-18 relative)
+    float psi_lo, pad0;          // low 32 bits of arg(c)/2pi 2^64, times 2^-64
     double a, b, d;
 };
 
@@ -90,21 +91,38 @@ MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandReg
         for (int q = 0; q < 3; ++q) sum[i][q] += (double)acc[i][q];
 }
 
+// sin/cos(2 pi y) for any y (turns): y = q/1024 + r with |r| <= 2^-11 (exact), the table
+// entry (cos, sin)(2 pi q/1024) rotated by r through short polynomials (truncation below 3e-15).
+constexpr int HEAVY_TAB = 1024;
+MB_DEV void sincos_turns_tab(double y, const double2 *tab, double &sn, double &cs) {
+    const double m = fma(y, (double)HEAVY_TAB, MB_MAGIC);
+    const int q = __double2loint(m) & (HEAVY_TAB - 1);
+    const double r = fma(-1.0 / HEAVY_TAB, m - MB_MAGIC, y);
+    const double u = r * r;
+    const double s = r * fma(u, -41.341702240399755, 6.283185307179586);     // sin(2 pi r)
+    const double cm1 = u * fma(u, 64.93939402266828, -19.739208802178716);  // cos(2 pi r) - 1
+    const double2 T = tab[q];
+    cs = fma(T.x, cm1, fma(-T.y, s, T.x));
+    sn = fma(T.y, cm1, fma(T.x, s, T.y));
+}
+
 template <int CPT>
 MB_DEV void heavy_tile(const ZHeavy *tile, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
-                       double (&acc)[CPT][3]) {
+                       double (&acc)[CPT][3], const double2 *tab) {
     for (int jj = zl; jj < nt; jj += ZL) {
         const ZHeavy z = tile[jj];
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
-            uint32_t lo32 = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi;
-            // the chain starts from psi = arg(c)/2pi, so the last product's DFMA also adds it
+            uint32_t lo32 = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi + z.psi_hi;
+            // the 2^-96 products (< 2^-30 turn in all) in FP32, seeded with psi's low word
+            const float low = fmaf(__uint2float_rn(cr[i].a1), z.c0f, fmaf(__uint2float_rn(cr[i].a0), z.c1f,
+                              fmaf(__uint2float_rn(cr[i].d1), z.b0f,
+                              fmaf(__uint2float_rn(cr[i].d0), z.b1f, z.psi_lo))));
             double F = fma(cr[i].A0, z.b0s, fma(cr[i].A1, z.c1s, fma(cr[i].D0, z.gis,
-                       fma(cr[i].D1, z.b1s, fma(cr[i].A1, z.c0t, fma(cr[i].A0, z.c1t,
-                       fma(cr[i].D1, z.b0t, fma(cr[i].D0, z.b1t, z.psi))))))));
+                       fma(cr[i].D1, z.b1s, (double)low))));
             double y = fma(u32_to_f64(lo32), TWO_M32, F);
             double sn, cs;
-            sincos_turns_quad(y, sn, cs);
+            sincos_turns_tab(y, tab, sn, cs);
             acc[i][0] = fma(z.a, cs, acc[i][0]);
             acc[i][1] = fma(z.b, sn, acc[i][1]);
             acc[i][2] = fma(z.d, cs, acc[i][2]);
@@ -134,17 +152,19 @@ MB_DEV void stage_heavy(const TabView &t, int64_t j, double k, const double *w, 
     double g = t.gamma[j];
     double a = 2.0 * t.alpha[j] * (w ? w[j] : exp(-k * g * g));
     uint32_t c0 = t.g0[j], c1 = t.g1[j], b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j];
-    r.b0 = b0; r.b1 = b1; r.gi = gi; r.pad = 0;
+    r.b0 = b0; r.b1 = b1; r.gi = gi;
     r.b0s = u32_to_f64(b0) * TWO_M64;
     r.c1s = u32_to_f64(c1) * TWO_M64;
     r.gis = u32_to_f64(gi) * TWO_M64;
     r.b1s = u32_to_f64(b1) * TWO_M64;
-    r.c0t = u32_to_f64(c0) * TWO_M96;
-    r.c1t = u32_to_f64(c1) * TWO_M96;
-    r.b0t = u32_to_f64(b0) * TWO_M96;
-    r.b1t = u32_to_f64(b1) * TWO_M96;
-    uint64_t ps = t.psi[j];
-    r.psi = fma(u32_to_f64((uint32_t)(ps >> 32)), TWO_M32, u32_to_f64((uint32_t)ps) * TWO_M64);
+    r.c0f = (float)(u32_to_f64(c0) * TWO_M96);
+    r.c1f = (float)(u32_to_f64(c1) * TWO_M96);
+    r.b0f = (float)(u32_to_f64(b0) * TWO_M96);
+    r.b1f = (float)(u32_to_f64(b1) * TWO_M96);
+    const uint64_t ps = t.psi[j];
+    r.psi_hi = (uint32_t)(ps >> 32);
+    r.psi_lo = (float)(u32_to_f64((uint32_t)ps) * TWO_M64);
+    r.pad0 = 0.f;
     r.a = a;
     r.b = -a * g;
     r.d = -a * g * g;
@@ -211,7 +231,7 @@ MB_DEV void light_item(const FastItem &it, const FastGroup &gr, const TabView &t
 
 template <int CPT>
 MB_DEV void heavy_item(const FastItem &it, const FastGroup &gr, const TabView &t, const CandView &c,
-                       double *partial, unsigned char *smem) {
+                       double *partial, unsigned char *smem, const double2 *tab) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nzw = it.nzw;
     const int cgroup = warp / nzw, zw = warp - cgroup * nzw;
@@ -229,7 +249,7 @@ MB_DEV void heavy_item(const FastItem &it, const FastGroup &gr, const TabView &t
         int64_t j = tb + threadIdx.x;
         if (threadIdx.x < HEAVY_TILE && j < it.z1) stage_heavy(t, j, gr.k, gr.w, tile[threadIdx.x]);
         __syncthreads();
-        heavy_tile<CPT>(tile, (int)min((int64_t)HEAVY_TILE, it.z1 - tb), zw, nzw, cr, res);
+        heavy_tile<CPT>(tile, (int)min((int64_t)HEAVY_TILE, it.z1 - tb), zw, nzw, cr, res, tab);
     }
     finish_item<CPT>(it, gr, res, warp, lane, zw, cbase, cend, partial, smem);
 }
@@ -240,7 +260,13 @@ __global__ void __launch_bounds__(FAST_THREADS, 2)
 k2_heavy_kernel(TabView t, CandView c, const FastItem *items, int n_items, const FastGroup *groups,
                 int *counter, double *partial) {
     __shared__ __align__(16) unsigned char smem[FAST_SMEM];
+    __shared__ double2 s_tab[HEAVY_TAB];
     __shared__ int s_item;
+    for (int i = threadIdx.x; i < HEAVY_TAB; i += FAST_THREADS) {
+        double sn, cs;
+        sincospi((double)i * (2.0 / HEAVY_TAB), &sn, &cs);
+        s_tab[i] = make_double2(cs, sn);
+    }
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -248,7 +274,7 @@ k2_heavy_kernel(TabView t, CandView c, const FastItem *items, int n_items, const
         const int idx = s_item;
         if (idx >= n_items) break;
         const FastItem it = items[idx];
-        heavy_item<HEAVY_CPT>(it, groups[it.group], t, c, partial, smem);
+        heavy_item<HEAVY_CPT>(it, groups[it.group], t, c, partial, smem, s_tab);
     }
 }
 

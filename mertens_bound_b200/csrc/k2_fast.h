@@ -50,7 +50,8 @@ struct FastPlanDev {
 //          the radians->turns product inside sin.approx, <= 2^-23 pi each) + phase 4.5 2^-32
 //          turn + amplitude and FFMA roundings (2 2^-24) + FP32 summation over a 16-term flush
 //          window (15 2^-24)  ->  2.2e-6
-//   heavy: phase 2^-47 turn, polynomial 5.6e-14, FP64 roundings  ->  2e-13
+//   heavy: phase 2^-47 turn, table + polynomial 3e-15, FP64 roundings  ->  2e-13 (kept loose:
+//          the heavy amplitude sum is O(1), so this share of the bound is negligible)
 constexpr double EPS_LIGHT = 2.2e-6;
 constexpr double EPS_HEAVY = 2.0e-13;
 

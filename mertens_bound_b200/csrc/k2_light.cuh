@@ -21,7 +21,7 @@ constexpr double TWO_M96 = 1.2621774483536189e-29;
 
 // Candidate registers of the light and heavy phases.
 struct CandRegs {
-    uint32_t a0, a1, d1;
+    uint32_t a0, a1, d1, d0;
     double A0, A1, D0, D1;      // exact doubles of the limbs a0, a1, d0, d1
 };
 
@@ -30,6 +30,7 @@ MB_DEV CandRegs cand_regs_of(Cand64 v) {
     r.a0 = (uint32_t)v.vi;
     r.a1 = (uint32_t)(v.vi >> 32);
     r.d1 = (uint32_t)(v.vf >> 32);
+    r.d0 = (uint32_t)v.vf;
     r.A0 = u32_to_f64(r.a0);
     r.A1 = u32_to_f64(r.a1);
     r.D0 = u32_to_f64((uint32_t)v.vf);
