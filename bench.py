@@ -47,9 +47,9 @@ WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 can
 # per launch on this workload, from the ncu capture of `bench.py --profile-case search`
 # summarised in profiles/k2_light_kernel_search_scoring.md.
 LIGHT_INST_PER_TERM = {2: 23.40, 3: 25.62, 4: 20.03}
-HEAVY_INST_PER_TERM = 53.94
+HEAVY_INST_PER_TERM = 41.09
 LIGHT_DRAM_BYTES = {2: 16487680, 3: 16466176, 4: 16446464}
-HEAVY_DRAM_BYTES = 2775040
+HEAVY_DRAM_BYTES = 2781952
 REF_SAMPLE_CANDS = 64
 
 
