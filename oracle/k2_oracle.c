@@ -13,6 +13,10 @@
  *   compute_peak_AB / polish_peaks_with_weights semantics
  *     -- search/path1_eval_fast.cpp:15-53 and :58-143 (restated in orc_ref_peak_AB /
  *        orc_ref_polish below, line for line in meaning, single-threaded).
+ *   The enumerators' CPU leaf screen ZeroData::fast_screen
+ *     -- search/fast_mertens_enum.cpp:99-104 (16384-entry FP32 cosine table, offset steps) and
+ *        :108-142 (two stages of 64 zeros, 7 offsets, thresholds 0.810 / 0.875), restated in
+ *        orc_fast_screen below, OpenMP over leaves as the enumerator runs it.
  *
  * Fixed-point conventions used throughout this repository:
  *   G = gamma/2pi as unsigned 64.128 fixed point: G = g_int + g_hi 2^-64 + g_lo 2^-128
@@ -230,4 +234,45 @@ void orc_ref_polish(int n_peaks, int n_zeros, const double *A, const double *B, 
         if (fabs(h0) > fabs(hf)) { out_h_pol[p] = h0; out_ddy_pol[p] = 0.0; }
         else { out_h_pol[p] = hf; out_ddy_pol[p] = ddy; }
     }
+}
+
+/* ZeroData::fast_screen over P leaves x (u128, the enumerators' x = floor(y 2^30)) on the
+ * reference's table layout; pass[p] = 1 when the leaf survives both stages.  Returns the number of
+ * passing leaves.  The cosine table and step indices are built per call as the reference builds
+ * them once per table (search/fast_mertens_enum.cpp:99-104; offset step 0.0014). */
+int64_t orc_fast_screen(int64_t P, const uint64_t *x_lo, const uint64_t *x_hi, const uint64_t *ghi_lo,
+                        const uint64_t *ghi_hi, const uint64_t *glo_lo, const uint64_t *glo_hi,
+                        const uint64_t *psi_lo, const uint64_t *psi_hi, const double *two_astar,
+                        const double *gamma, uint8_t *pass) {
+    static float lut[16384];
+    uint32_t st[128];
+    for (int k = 0; k < 16384; ++k) lut[k] = (float)cos(2.0 * M_PI * (double)k / 16384.0);
+    for (int i = 0; i < 128; ++i)
+        st[i] = ((uint32_t)llround(gamma[i] * 0.0014 * (16384.0 / (2.0 * M_PI)))) & 16383u;
+    int64_t n_pass = 0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : n_pass)
+    for (int64_t p = 0; p < P; ++p) {
+        const u128 x = ((u128)x_hi[p] << 64) | x_lo[p];
+        const uint64_t xh = (uint64_t)(x >> 48);
+        const uint64_t xl = (uint64_t)(x & (((u128)1 << 48) - 1));
+        float s[7] = {0, 0, 0, 0, 0, 0, 0};
+        int ok = 1;
+        for (int stage = 0; stage < 2 && ok; ++stage) {
+            for (int i = 64 * stage; i < 64 * stage + 64; ++i) {
+                const u128 ghi = ((u128)ghi_hi[i] << 64) | ghi_lo[i];
+                const u128 glo = ((u128)glo_hi[i] << 64) | glo_lo[i];
+                const u128 psi = ((u128)psi_hi[i] << 64) | psi_lo[i];
+                const u128 ph = (u128)xh * ghi + (u128)xl * glo - psi;
+                const uint32_t i0 = (uint32_t)((uint64_t)(ph >> 64) >> 50);
+                const float w = (float)two_astar[i];
+                for (int m = -3; m <= 3; ++m) s[m + 3] += w * lut[(i0 + (uint32_t)m * st[i]) & 16383u];
+            }
+            float mx = 0.f;
+            for (int m = 0; m < 7; ++m) mx = fmaxf(mx, fabsf(s[m]));
+            ok = mx >= (stage == 0 ? 0.810f : 0.875f);
+        }
+        pass[p] = (uint8_t)ok;
+        n_pass += ok;
+    }
+    return n_pass;
 }

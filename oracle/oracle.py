@@ -14,6 +14,7 @@ Contents
                            search/eval_tech1_600k.py:213-215).
   * polish_ref          -- (module oracle.polish_ref) numpy restatement of the per-peak polishes of
                            search/path1_kernel_opt.py.
+  * Oracle.fast_screen  -- restated ZeroData::fast_screen (search/fast_mertens_enum.cpp:108-142).
   * RefLib              -- binding of _ref/libpath1_eval.so, the reference's own evaluator
                            compiled from search/path1_eval_fast.cpp (see Makefile).
 """
@@ -70,6 +71,8 @@ class Oracle:
         L.orc_gamma_from_G.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
         L.orc_ref_peak_AB.argtypes = [C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 11
         L.orc_ref_polish.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_double, C.c_int] + [C.c_void_p] * 3
+        L.orc_fast_screen.argtypes = [C.c_int64] + [C.c_void_p] * 11
+        L.orc_fast_screen.restype = C.c_int64
         self.L = L
 
     def phase128(self, cands, G3, n=None):
@@ -136,6 +139,19 @@ class Oracle:
                                _p(reft["psi_lo"]), _p(reft["psi_hi"]), _p(A), _p(B),
                                _p(top) if want_top else None)
         return (A, B, top) if want_top else (A, B)
+
+    def fast_screen(self, x_lo, x_hi, reft, two_astar):
+        """Restated ZeroData::fast_screen (search/fast_mertens_enum.cpp:108-142) over leaves
+        x = x_hi 2^64 + x_lo on the reference layout; returns the per-leaf pass flags."""
+        x_lo = np.ascontiguousarray(x_lo, dtype=np.uint64)
+        x_hi = np.ascontiguousarray(x_hi, dtype=np.uint64)
+        ta = np.ascontiguousarray(two_astar[:128], dtype=np.float64)
+        g = np.ascontiguousarray(reft["gamma"][:128], dtype=np.float64)
+        out = np.zeros(x_lo.shape[0], dtype=np.uint8)
+        self.L.orc_fast_screen(x_lo.shape[0], _p(x_lo), _p(x_hi), _p(reft["ghi_lo"]), _p(reft["ghi_hi"]),
+                               _p(reft["glo_lo"]), _p(reft["glo_hi"]), _p(reft["psi_lo"]), _p(reft["psi_hi"]),
+                               _p(ta), _p(g), _p(out))
+        return out
 
     def ref_polish(self, A, B, gamma, w, half, steps):
         P, n = A.shape

@@ -7,6 +7,10 @@ import time), so its two polish functions are restated from their published beha
   polish_single_peak      search/path1_kernel_opt.py:94-147
   fast_polish_batch_blas  search/path1_kernel_opt.py:150-221
 
+and the FP64 grid of search/polish.py's scan (:50-72; its mpfr phase reduction is the caller's):
+
+  scan_grid
+
 Both work on caller A/B rows; the numerics are plain FP64 numpy, as in the reference.  The
 restatement differs from the reference only in the top-peak order on exact ties of |h_pol|
 (index order here; numpy's default argsort leaves it unspecified).
@@ -92,3 +96,16 @@ def fast_polish_batch(A_mat, B_mat, gamma_vec, w_vec, ddy_grid=None, top=25):
         else:
             h_pol[i], ddy_pol[i] = h_unpol[i], 0.0
     return h_unpol, h_pol, ddy_pol
+
+
+def scan_grid(phi, dphi, gre, gim, m0, m1, chunk=4000):
+    """h(y0 + m step) for m in [m0, m1) as search/polish.py:60-66 forms it: angles
+    phi + m dphi in FP64 (phi = gamma y0 mod 2pi, dphi = gamma step mod 2pi), chunks of `chunk`
+    grid points, h = 2 sum(gre cos - gim sin) with (gre, gim) = e^{-k gamma^2} (Re c, Im c)."""
+    out = []
+    for a in range(m0, m1, chunk):
+        b = min(a + chunk, m1)
+        m = np.arange(a, b, dtype=np.float64)[:, None]
+        ang = phi[None, :] + m * dphi[None, :]
+        out.append(2.0 * np.sum(gre * np.cos(ang) - gim * np.sin(ang), axis=1))
+    return np.concatenate(out) if out else np.empty(0)

@@ -86,3 +86,44 @@ def test_reference_phase_reduction_restated(oracle, small_table):
             want = ((((int(hi[p, j]) << 64) | int(lo[p, j])) - psi) % (1 << 128)) >> 64
             d = (int(top[p, j]) - want) % (1 << 64)
             assert d in (0, 1, (1 << 64) - 1)
+
+
+def test_fast_screen_restatement(oracle):
+    """The C restatement of ZeroData::fast_screen (search/fast_mertens_enum.cpp:99-142) against a
+    pure-Python one: u128 phase, 14-bit index into the FP32 cosine table, seven offsets, FP32
+    sums in the reference's order, stage thresholds 0.810 / 0.875.  The amplitudes are scaled up
+    so that leaves pass, fail at the first stage and fail at the second."""
+    import math
+    d = synth.make_table(2000, seed=3)
+    reft = reference_format(d, exact_psi=False)
+    ta = 4.0 * 2.0 * reft["alpha"] * np.exp(-3e-9 * d.gamma ** 2)
+    rng = np.random.default_rng(1)
+    xs = [int(rng.integers(3_400_000_000_000_000_000, 3_600_000_000_000_000_000)) << 30 |
+          int(rng.integers(0, 1 << 30)) for _ in range(160)]
+    flags = oracle.fast_screen(np.array([x & MASK64 for x in xs], np.uint64),
+                               np.array([x >> 64 for x in xs], np.uint64), reft, ta)
+    f32 = np.float32
+    lut = np.array([math.cos(2.0 * math.pi * k / 16384.0) for k in range(16384)]).astype(np.float32)
+    st = [int(round(g * 0.0014 * (16384.0 / (2.0 * math.pi)))) & 16383 for g in d.gamma[:128]]
+    limbs = [((int(reft["ghi_hi"][i]) << 64) | int(reft["ghi_lo"][i]),
+              (int(reft["glo_hi"][i]) << 64) | int(reft["glo_lo"][i]),
+              (int(reft["psi_hi"][i]) << 64) | int(reft["psi_lo"][i])) for i in range(128)]
+
+    def screen(x):
+        xh, xl = x >> 48, x & ((1 << 48) - 1)
+        s = [f32(0)] * 7
+        for stage, thr in ((0, f32(0.810)), (1, f32(0.875))):
+            for i in range(64 * stage, 64 * stage + 64):
+                ghi, glo, psi = limbs[i]
+                i0 = ((xh * ghi + xl * glo - psi) % (1 << 128)) >> 114
+                w = f32(ta[i])
+                for m in range(7):
+                    s[m] = f32(s[m] + f32(w * lut[(i0 + (m - 3) * st[i]) % 16384]))
+            if max(abs(v) for v in s) < thr:
+                return 0, stage
+        return 1, 2
+
+    res = [screen(x) for x in xs]
+    assert [r[0] for r in res] == flags.tolist()
+    outcomes = {r[1] for r in res}
+    assert outcomes == {0, 1, 2}, outcomes
