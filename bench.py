@@ -387,6 +387,100 @@ def certified_cpu_rate(big, pk, n_full: int, per_worker: int = 1500):
                       "restating certify_K2.work; python-flint is not installed"}
 
 
+_HP = {}
+
+
+def _hp_init(ta, gamma):
+    _HP["ta"], _HP["gamma"] = ta, gamma
+
+
+def _hp_one(top):
+    """One hit through the restated ZeroData::polish, all five stages (no early exit)."""
+    from oracle.oracle import zerodata_polish
+    zerodata_polish(top, _HP["ta"], _HP["gamma"], thresholds=(None, None, None))
+    return 1
+
+
+def _hp_warm(_):
+    import oracle.oracle  # noqa: F401
+    return 0
+
+
+def screen_cpu(reft, two_astar, pts):
+    """Leaves/s of the enumerators' CPU screen ZeroData::fast_screen (C restatement in the oracle,
+    OpenMP over leaves on all host cores as the enumerator runs it) on the same leaves; x =
+    floor(v 2^30) as the enumerators hold them."""
+    from oracle.oracle import Oracle
+    vi, vf = pts[:, 0].astype(np.uint64), pts[:, 1].astype(np.uint64)
+    x_lo = (vi << np.uint64(30)) | (vf >> np.uint64(34))
+    x_hi = vi >> np.uint64(34)
+    O = Oracle()
+    O.fast_screen(x_lo[:4096], x_hi[:4096], reft, two_astar)
+    t0 = time.perf_counter()
+    flags = O.fast_screen(x_lo, x_hi, reft, two_astar)
+    secs = time.perf_counter() - t0
+    return {"kind": "port", "cores": os.cpu_count(), "leaves": int(len(x_lo)), "seconds": secs,
+            "leaves_per_s": len(x_lo) / secs, "passed": int(flags.sum()),
+            "sample": "all leaves; ZeroData::fast_screen restated in C (64 + 64 zeros, 14-bit FP32 cosine "
+                      "table, 7 offsets, thresholds 0.810 / 0.875)"}
+
+
+def hit_polish_cpu(d600, hits, reft):
+    """Hits/s of ZeroData::polish on the host cores: the numpy restatement of
+    search/gpu_mertens_stream.cu:381-505 (all five stages, every hit to the end), one hit per core
+    in a spawn pool; the reference runs the same stages in C++ with OpenMP over hits.  The hits'
+    phase words come from the restated compute_peak_AB on the reference's table layout."""
+    import multiprocessing as mp
+    from oracle.oracle import MASK64, Oracle
+    n = os.cpu_count() or 1
+    x = [(int(a) << 30) | (int(b) >> 34) for a, b in hits[:n]]
+    x_lo = np.array([v & MASK64 for v in x], np.uint64)
+    x_hi = np.array([v >> 64 for v in x], np.uint64)
+    _, _, top = Oracle().ref_peak_AB((x_lo, x_hi, np.zeros(len(x))), reft, want_top=True)
+    ta = 2.0 * reft["alpha"] * np.exp(-3e-9 * d600.gamma ** 2)
+    try:
+        with mp.get_context("spawn").Pool(n, initializer=_hp_init, initargs=(ta, d600.gamma)) as pool:
+            pool.map_async(_hp_warm, range(n), chunksize=1).get(timeout=300)
+            t0 = time.perf_counter()
+            done = sum(pool.map_async(_hp_one, [row.view(np.int64) for row in top], chunksize=1).get(timeout=600))
+            secs = time.perf_counter() - t0
+    except Exception as e:                                       # a worker failed or timed out
+        return {"kind": "port", "unavailable": f"{type(e).__name__}: {e}"}
+    return {"kind": "port", "cores": n, "hits": done, "seconds": secs, "hits_per_s": done / secs,
+            "sample": f"{done} of the same hits, one per core; numpy restatement of ZeroData::polish "
+                      "(oracle.zerodata_polish), phase words from the restated compute_peak_AB"}
+
+
+def polish_scan_cpu(t74, n74, m_half: int = 200):
+    """Point-zero terms/s of search/polish.py's FP64 grid (oracle.polish_ref.scan_grid: angles
+    phi + m dphi, cos and sin per term, numpy on one core as in the reference) on 2 m_half points of
+    the same scan; phi and dphi are the exact phases (polish.py reduces them with mpfr, untimed
+    here as there)."""
+    from fractions import Fraction
+    from mertens_bound_b200 import polish, synth
+    from oracle.oracle import Oracle
+    from oracle.polish_ref import scan_grid
+    O = Oracle()
+    G3 = t74.G3[:n74]
+    vi, vf = polish.to_fixed(synth.PEAK2_STR)
+    si, sf = polish.to_fixed(Fraction(2e-5))
+    two_pi = 2.0 * math.pi
+    ph = O.phase128(synth.Candidates(np.array([vi], np.uint64), np.array([vf], np.uint64), np.zeros(1)), G3, n74)[0]
+    dp = O.phase128(synth.Candidates(np.array([si], np.uint64), np.array([sf], np.uint64), np.zeros(1)), G3, n74)[0]
+    phi = ph[0].astype(np.float64) * (two_pi / 2.0 ** 64)
+    dphi = dp[0].astype(np.float64) * (two_pi / 2.0 ** 64)
+    w = np.exp(-3e-9 * t74.gamma[:n74] ** 2)
+    gre, gim = w * t74.c_re[:n74], w * t74.c_im[:n74]
+    t0 = time.perf_counter()
+    scan_grid(phi, dphi, gre, gim, -m_half, m_half, chunk=2 * m_half)
+    secs = time.perf_counter() - t0
+    terms = 2 * m_half * n74
+    return {"kind": "port", "cores": 1, "points": 2 * m_half, "seconds": secs,
+            "point_zero_terms_per_s": terms / secs,
+            "sample": f"{2 * m_half} of the 25,001 grid points over all {n74} zeros, one chunk "
+                      "(polish.py uses chunks of 4,000 points)"}
+
+
 def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
     """The other four workload shapes, measured briefly on the same GPU (summary numbers)."""
     from mertens_bound_b200 import k2, synth, _lib
@@ -540,6 +634,15 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
         out["enumerator_screen"] = {"leaves": len(pts), "seconds": sc_s, "leaves_per_s": len(pts) / sc_s,
                                     "hits": int(len(r.hits)), "stages": "64/128/256 zeros, 0.78/0.855/0.892",
                                     "note": "host-pointer call: includes the H2D of 16 MB of leaves"}
+        reft = None
+        if cpu_baseline:
+            try:
+                from oracle.oracle import reference_format
+                reft = reference_format(d600, exact_psi=False)
+                ta600 = 2.0 * reft["alpha"] * np.exp(-3e-9 * d600.gamma ** 2)
+                out["enumerator_screen"]["cpu_baseline"] = screen_cpu(reft, ta600, pts)
+            except Exception as e:                                   # the baseline is optional
+                out["enumerator_screen"]["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
         hits = pts[:256]
         hit_polish.polish_hits(t6, hits[:8])
         t0 = time.perf_counter()
@@ -547,6 +650,8 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
         hp_s = time.perf_counter() - t0
         out["hit_polish"] = {"hits": 256, "zeros": d600.n, "seconds": hp_s, "hits_per_s": 256 / hp_s,
                              "stages_run": int(hr.stage.max()) + 1, "thresholds": "none (every hit runs all stages)"}
+        if reft is not None:
+            out["hit_polish"]["cpu_baseline"] = hit_polish_cpu(d600, hits, reft)
         n74 = t6.count_below(polish.POLISH_T)
         polish.scan(t6, synth.PEAK2_STR, 0.001, 2e-5)
         t0 = time.perf_counter()
@@ -554,6 +659,11 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
         ps_s = time.perf_counter() - t0
         out["polish_scan"] = {"points": 25001, "zeros": n74, "seconds": ps_s,
                               "point_zero_terms_per_s": 25001 * n74 / ps_s, "best_abs_h": abs(best)}
+        if cpu_baseline:
+            try:
+                out["polish_scan"]["cpu_baseline"] = polish_scan_cpu(d600, n74)
+            except Exception as e:                                   # the baseline is optional
+                out["polish_scan"]["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
 
     # taylor_polish: search/path1_kernel_opt.py's fast_polish_batch_blas contract (degree-16
     # moments, 121-point grid, exact Newton on the top 25) for 1,024 candidates over its 100,000
