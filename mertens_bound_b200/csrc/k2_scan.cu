@@ -3,8 +3,11 @@
 // mod 2pi).  Here step is a 64.64 fixed-point number and the phase of every grid point is exact:
 //   frac(y_m G) = frac(frac(v G) + m frac(step G))     (128-bit words, mod 1)
 // Each thread takes MPT consecutive grid points: one 128 x 32-bit product per zero gives the
-// first, 128-bit additions give the rest.  Sine/cosine in FP64 (quarter-turn polynomials), FP64
-// accumulation, deterministic reduction over zero chunks.
+// exact phase of the first, whose sine/cosine (FP64, quarter-turn polynomials) times the
+// amplitude is rotated to the other MPT - 1 points by powers of (cos, sin)(2 pi frac(step G)) of
+// that zero (the reference's angle addition, polish.py:60-66, gpu_mertens_stream.cu:324-356,
+// anchored afresh at an exact phase every MPT points; each point at most four rotations from its
+// anchor).  FP64 accumulation, deterministic reduction over zero chunks.
 #include <algorithm>
 #include <cmath>
 
@@ -15,14 +18,53 @@ namespace mb {
 namespace {
 
 constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_MPT = 8;                     // grid points per thread
+constexpr int SCAN_MPT = 16;                    // grid points per thread (one exact anchor)
+static_assert(SCAN_MPT == 16, "add_rotations16 covers 16 points");
 constexpr int SCAN_TILE = 256;                  // zeros per staged tile
 struct __align__(16) ZScan {
     uint64_t p_lo, p_hi;       // frac(v G) + psi, 2^-128 units
     uint64_t d_lo, d_hi;       // frac(step G), 2^-128 units
     double a;                  // 2 |c| exp(-k gamma^2)
+    double rc[4], rs[4];       // cos, sin of 2^b 2 pi frac(step G), b = 0..3
     double pad;
 };
+
+// (c, s) rotated by the angle whose cosine and sine are (cd, sd)
+MB_DEV void rot(double c, double s, double cd, double sd, double &oc, double &os) {
+    oc = fma(c, cd, -s * sd);
+    os = fma(s, cd, c * sd);
+}
+
+// acc[i] += Re((c + i s) e^{i i phi}) for i = 0..15, given (rc[b], rs[b]) = (cos, sin)(2^b phi):
+// a rotation tree of depth 4 (z8 from z0, z4 and z12, then the even points, then the odd ones,
+// which need only their cosine), so every point is at most four rotations from the exact anchor
+// and the chains are independent.
+MB_DEV void add_rotations16(double c0, double s0, const double (&rc)[4], const double (&rs)[4], double (&acc)[16]) {
+    double c[16], s[16];
+    c[0] = c0;
+    s[0] = s0;
+    rot(c[0], s[0], rc[3], rs[3], c[8], s[8]);
+#pragma unroll
+    for (int i = 0; i < 16; i += 8) rot(c[i], s[i], rc[2], rs[2], c[i + 4], s[i + 4]);
+#pragma unroll
+    for (int i = 0; i < 16; i += 4) rot(c[i], s[i], rc[1], rs[1], c[i + 2], s[i + 2]);
+#pragma unroll
+    for (int i = 0; i < 16; i += 2) {
+        acc[i] += c[i];
+        acc[i + 1] += fma(c[i], rc[0], -s[i] * rs[0]);
+    }
+}
+
+// (cos, sin)(2^b phi), b = 0..3, from (cos, sin)(phi) by repeated squaring
+MB_DEV void rotation_powers(double cd, double sd, double (&rc)[4], double (&rs)[4]) {
+    rc[0] = cd;
+    rs[0] = sd;
+#pragma unroll
+    for (int b = 1; b < 4; ++b) {
+        rc[b] = fma(rc[b - 1], rc[b - 1], -rs[b - 1] * rs[b - 1]);
+        rs[b] = 2.0 * rc[b - 1] * rs[b - 1];
+    }
+}
 
 // partial[((p * n_chunk) + chunk) * n_m + m]
 __global__ void __launch_bounds__(SCAN_THREADS)
@@ -55,6 +97,9 @@ k2_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, u
             r.d_hi = hi;
             const double g = t.gamma[j];
             r.a = 2.0 * t.alpha[j] * exp(-k * g * g);
+            double cd, sd;
+            sincospi(2.0 * s64_turns_to_f64(hi), &sd, &cd);   // ~1 ulp: errors add up over the rotations
+            rotation_powers(cd, sd, r.rc, r.rs);
             r.pad = 0.0;
             tile[threadIdx.x] = r;
         }
@@ -70,18 +115,11 @@ k2_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, u
                 mlo = ~mlo + 1;
                 mhi = ~mhi + (mlo == 0 ? 1 : 0);
             }
-            uint64_t xlo = z.p_lo + mlo;
-            uint64_t xhi = z.p_hi + mhi + (xlo < mlo ? 1 : 0);
-#pragma unroll
-            for (int i = 0; i < SCAN_MPT; ++i) {
-                const double y = s64_turns_to_f64(xhi);
-                double sn, cs;
-                sincos_turns_quad(y, sn, cs);
-                acc[i] = fma(z.a, cs, acc[i]);
-                const uint64_t nlo = xlo + z.d_lo;
-                xhi = xhi + z.d_hi + (nlo < xlo ? 1 : 0);
-                xlo = nlo;
-            }
+            const uint64_t xlo = z.p_lo + mlo;
+            const uint64_t xhi = z.p_hi + mhi + (xlo < mlo ? 1 : 0);
+            double sn, cs;
+            sincos_turns_quad(s64_turns_to_f64(xhi), sn, cs);
+            add_rotations16(cs * z.a, sn * z.a, z.rc, z.rs, acc);
         }
     }
     if (mb < n_m) {
@@ -93,11 +131,17 @@ k2_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, u
 }
 
 // Small grids over many base points (the hit polish of the enumerators): one CTA per base point,
-// threads over zeros; for each zero the exact phase at the base point and the exact increment
-// per grid step, then every grid point in turn: warp-shuffle sum of the 32 lanes' terms, added
-// by lane 0 to its warp's row of shared accumulators (fixed order -> deterministic).
+// each thread HIT_ZPT zeros per round.  Per zero: the exact phase at the grid's first point and
+// the exact increment per step; every HIT_MB points an exact anchor (FP64 sine/cosine of the
+// 128-bit phase, times the amplitude), rotated to the points in between by powers of the
+// increment's (cos, sin).  A block of HIT_MB points is summed over the thread's zeros, then over
+// the warp by a fixed shuffle tree, and lane 0 adds it to its warp's row of shared accumulators
+// (fixed order -> deterministic).
 constexpr int HIT_THREADS = 256;
 constexpr int HIT_MAX_M = 1024;
+constexpr int HIT_ZPT = 2;
+constexpr int HIT_MB = 16;
+static_assert(HIT_MB == 16, "add_rotations16 and the anchor step (increment << 4) assume 16");
 
 __global__ void __launch_bounds__(HIT_THREADS)
 k2_hit_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, uint64_t sf, int64_t m0, int n_m,
@@ -109,42 +153,62 @@ k2_hit_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t s
     __syncthreads();
     const uint64_t a_int = vi[p], a_frac = vf[p];
     const uint32_t mabs = (uint32_t)(m0 < 0 ? -m0 : m0);
-    const int64_t rounds = (n_use + HIT_THREADS - 1) / HIT_THREADS;
+    constexpr int PER_ROUND = HIT_THREADS * HIT_ZPT;
+    const int64_t rounds = (n_use + PER_ROUND - 1) / PER_ROUND;
     for (int64_t r = 0; r < rounds; ++r) {
-        const int64_t j = r * HIT_THREADS + threadIdx.x;
-        const bool live = j < n_use;
-        uint64_t xlo = 0, xhi = 0, dlo = 0, dhi = 0;
-        double a = 0.0;
-        if (live) {
-            uint64_t hi, lo;
-            phase128_exact((uint32_t)a_frac, (uint32_t)(a_frac >> 32), (uint32_t)a_int, (uint32_t)(a_int >> 32),
-                           t.g0[j], t.g1[j], t.g2[j], t.g3[j], t.g4[j], hi, lo);
-            const uint64_t plo = lo, phi = hi + t.psi[j];
-            phase128_exact((uint32_t)sf, (uint32_t)(sf >> 32), (uint32_t)si, (uint32_t)(si >> 32), t.g0[j], t.g1[j],
-                           t.g2[j], t.g3[j], t.g4[j], dhi, dlo);
-            uint64_t mlo = (uint64_t)mabs * dlo;
-            uint64_t mhi = __umul64hi((uint64_t)mabs, dlo) + (uint64_t)mabs * dhi;
-            if (m0 < 0) {
-                mlo = ~mlo + 1;
-                mhi = ~mhi + (mlo == 0 ? 1 : 0);
+        uint64_t xlo[HIT_ZPT], xhi[HIT_ZPT], dlo[HIT_ZPT], dhi[HIT_ZPT];
+        double a[HIT_ZPT], rc[HIT_ZPT][4], rs[HIT_ZPT][4];
+#pragma unroll
+        for (int z = 0; z < HIT_ZPT; ++z) {
+            const int64_t j = r * PER_ROUND + z * HIT_THREADS + threadIdx.x;
+            xlo[z] = xhi[z] = dlo[z] = dhi[z] = 0;
+            a[z] = 0.0;
+            double cd = 1.0, sd = 0.0;
+            if (j < n_use) {
+                uint64_t hi, lo;
+                phase128_exact((uint32_t)a_frac, (uint32_t)(a_frac >> 32), (uint32_t)a_int, (uint32_t)(a_int >> 32),
+                               t.g0[j], t.g1[j], t.g2[j], t.g3[j], t.g4[j], hi, lo);
+                const uint64_t plo = lo, phi = hi + t.psi[j];
+                phase128_exact((uint32_t)sf, (uint32_t)(sf >> 32), (uint32_t)si, (uint32_t)(si >> 32), t.g0[j],
+                               t.g1[j], t.g2[j], t.g3[j], t.g4[j], dhi[z], dlo[z]);
+                uint64_t mlo = (uint64_t)mabs * dlo[z];
+                uint64_t mhi = __umul64hi((uint64_t)mabs, dlo[z]) + (uint64_t)mabs * dhi[z];
+                if (m0 < 0) {
+                    mlo = ~mlo + 1;
+                    mhi = ~mhi + (mlo == 0 ? 1 : 0);
+                }
+                xlo[z] = plo + mlo;
+                xhi[z] = phi + mhi + (xlo[z] < mlo ? 1 : 0);
+                const double g = t.gamma[j];
+                a[z] = 2.0 * t.alpha[j] * exp(-k * g * g);
+                sincospi(2.0 * s64_turns_to_f64(dhi[z]), &sd, &cd);   // ~1 ulp: errors add up over the rotations
+                // the anchors advance by HIT_MB steps: d <<= log2(HIT_MB) (mod 2^128)
+                dhi[z] = (dhi[z] << 4) | (dlo[z] >> 60);
+                dlo[z] <<= 4;
             }
-            xlo = plo + mlo;
-            xhi = phi + mhi + (xlo < mlo ? 1 : 0);
-            const double g = t.gamma[j];
-            a = 2.0 * t.alpha[j] * exp(-k * g * g);
+            rotation_powers(cd, sd, rc[z], rs[z]);
         }
-        for (int m = 0; m < n_m; ++m) {
-            double v = 0.0;
-            if (live) {
+        for (int mb = 0; mb < n_m; mb += HIT_MB) {
+            double v[HIT_MB];
+#pragma unroll
+            for (int i = 0; i < HIT_MB; ++i) v[i] = 0.0;
+#pragma unroll
+            for (int z = 0; z < HIT_ZPT; ++z) {
                 double sn, cs;
-                sincos_turns_quad(s64_turns_to_f64(xhi), sn, cs);
-                v = a * cs;
-                const uint64_t nlo = xlo + dlo;
-                xhi = xhi + dhi + (nlo < xlo ? 1 : 0);
-                xlo = nlo;
+                sincos_turns_quad(s64_turns_to_f64(xhi[z]), sn, cs);
+                add_rotations16(cs * a[z], sn * a[z], rc[z], rs[z], v);
+                const uint64_t nlo = xlo[z] + dlo[z];
+                xhi[z] = xhi[z] + dhi[z] + (nlo < xlo[z] ? 1 : 0);
+                xlo[z] = nlo;
             }
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) acc[warp * n_m + m] += v;
+#pragma unroll
+            for (int i = 0; i < HIT_MB; ++i)
+                for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+            if (lane == 0) {
+#pragma unroll
+                for (int i = 0; i < HIT_MB; ++i)
+                    if (mb + i < n_m) acc[warp * n_m + mb + i] += v[i];
+            }
         }
     }
     __syncthreads();
