@@ -285,6 +285,16 @@ int mb_polish_single_exact(mb_table *t, int64_t P, const uint64_t *v_int, const 
 int mb_polish_peaks_exact(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                           const double *delta, int64_t n_zeros, int weight_slot, double grid_half_width,
                           int grid_steps, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);
+/* mb_polish_peaks_exact under n_weights registered weight vectors at once (outputs n_weights x P,
+ * row w for weight_slots[w]; each row equals the single-weight call).  The search drivers' step
+ * (search/eval_tech1_600k.py:216-273: compute_peak_AB once, then polish_peaks_with_weights per
+ * weight vector): the exact (A, B) of up to 65,535 peaks at a time is written once to a device
+ * buffer of at most 4 GiB, allocated for the call and freed before it returns, and read by every
+ * weight's polish. */
+int mb_polish_peaks_weights(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                            const double *delta, int64_t n_zeros, int n_weights, const int *weight_slots,
+                            double grid_half_width, int grid_steps, double *out_h_unpol, double *out_h_pol,
+                            double *out_ddy_pol);
 int mb_fast_polish_exact(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                          const double *delta, int64_t n_zeros, int weight_slot, const double *ddy_grid,
                          int64_t n_grid, int top, double *out_h_unpol, double *out_h_pol, double *out_ddy_pol);

@@ -316,6 +316,75 @@ extern "C" int mb_polish_peaks_exact(mb_table *h, int64_t P, const uint64_t *v_i
     return fetch_outputs(t.stream, P, s.hu, s.hp, s.dp, out_h_unpol, out_h_pol, out_ddy_pol);
 }
 
+// polish_peaks_with_weights under several weight vectors: the exact (A, B) of a chunk of peaks is
+// written once to HBM (the reference's P x N matrices, search/eval_tech1_600k.py:216-273, with the
+// exact phase of mb_exact_AB) and every weight's polish reads it, instead of recomputing each term's
+// 128-bit phase and sine/cosine in every pass.  Chunks keep the matrices within AB_BUDGET bytes.
+constexpr size_t AB_BUDGET = (size_t)4 << 30;
+
+extern "C" int mb_polish_peaks_weights(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                                       const double *delta, int64_t n_zeros, int n_weights, const int *weight_slots,
+                                       double grid_half_width, int grid_steps, double *out_h_unpol,
+                                       double *out_h_pol, double *out_ddy_pol) {
+    const char *who = "mb_polish_peaks_weights";
+    MB_CHECK_ARG(h && weight_slots && out_h_unpol && out_h_pol && out_ddy_pol, "%s: null argument", who);
+    MB_CHECK_ARG(n_weights >= 1 && n_weights <= 64, "%s: n_weights=%d (1..64)", who, n_weights);
+    MB_CHECK_ARG(P <= MAX_POLISH_PEAKS, "%s: P=%lld above %lld peaks per call", who, (long long)P,
+                 (long long)MAX_POLISH_PEAKS);
+    Table &t = table_of(h);
+    MB_TRY(check_peaks(t, P, v_int, v_frac, delta, n_zeros, who));
+    for (int w = 0; w < n_weights; ++w) MB_TRY(check_weights(t, weight_slots[w], who));
+    MB_CHECK_ARG(grid_steps >= 0 && grid_steps <= (1 << 19) && std::isfinite(grid_half_width), "%s: bad grid", who);
+    if (P == 0) return MB_OK;
+    if (n_zeros == 0) {                                  // nothing to hold: the per-weight form
+        for (int w = 0; w < n_weights; ++w)
+            MB_TRY(mb_polish_peaks_exact(h, P, v_int, v_frac, delta, 0, weight_slots[w], grid_half_width,
+                                         grid_steps, out_h_unpol + w * P, out_h_pol + w * P, out_ddy_pol + w * P));
+        return MB_OK;
+    }
+    MB_TRY(device_guard(t.device));
+    ExactStage s;
+    MB_TRY(stage_exact(t, P, v_int, v_frac, delta, nullptr, 0, 0, s));
+    const int64_t chunk =
+        std::max<int64_t>(1, std::min<int64_t>({P, (int64_t)65535, (int64_t)(AB_BUDGET / (16 * (size_t)n_zeros))}));
+    const size_t out_b = (size_t)n_weights * P * 8;
+    DevBuf buf;
+    MB_TRY(buf.ensure(2 * ((size_t)chunk * n_zeros * 8 + 256) + 3 * (out_b + 256)));
+    char *q = (char *)buf.p;
+    double *A = carve<double>(q, chunk * n_zeros);
+    double *B = carve<double>(q, chunk * n_zeros);
+    double *hu = carve<double>(q, (int64_t)n_weights * P);
+    double *hp = carve<double>(q, (int64_t)n_weights * P);
+    double *dp = carve<double>(q, (int64_t)n_weights * P);
+    const ABExact ex{view(t), s.vi, s.vf, s.delta};
+    cudaError_t e = cudaSuccess;
+    for (int64_t c0 = 0; c0 < P && e == cudaSuccess; c0 += chunk) {
+        const int64_t cn = std::min(chunk, P - c0);
+        exact_ab_kernel<<<dim3((unsigned)((n_zeros + 255) / 256), (unsigned)cn), 256, 0, t.stream>>>(ex, n_zeros, c0,
+                                                                                                     A, B);
+        e = cudaGetLastError();
+        for (int w = 0; w < n_weights && e == cudaSuccess; ++w) {
+            const int64_t o = (int64_t)w * P + c0;
+            PolishArgs a{n_zeros, t.d_gamma, t.d_weights[weight_slots[w]], nullptr, grid_steps, grid_half_width,
+                         nullptr, hu + o, hp + o, dp + o};
+            peak_polish_kernel<ABMatrix, POLISH_EVAL_FAST>
+                <<<(unsigned)(cn * POLISH_CLUSTER), POLISH_THREADS, 0, t.stream>>>(ABMatrix{A, B, n_zeros}, a);
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_h_unpol, hu, out_b, cudaMemcpyDeviceToHost, t.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_h_pol, hp, out_b, cudaMemcpyDeviceToHost, t.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_ddy_pol, dp, out_b, cudaMemcpyDeviceToHost, t.stream);
+    const cudaError_t es = cudaStreamSynchronize(t.stream);       // nothing in flight before the free
+    if (e == cudaSuccess) e = es;
+    buf.release();
+    if (e != cudaSuccess) {
+        set_error("%s: %s", who, cudaGetErrorString(e));
+        return MB_ERR_CUDA;
+    }
+    return MB_OK;
+}
+
 extern "C" int mb_fast_polish_exact(mb_table *h, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                                     const double *delta, int64_t n_zeros, int weight_slot, const double *ddy_grid,
                                     int64_t n_grid, int top, double *out_h_unpol, double *out_h_pol,

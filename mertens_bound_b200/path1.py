@@ -128,3 +128,19 @@ def polish_peaks_exact(table, cands, weight_slot: int, n_zeros: int | None = Non
     check(_lib.lib().mb_polish_peaks_exact(table.handle, P, ptr(vi), ptr(vf), ptr(d), n, int(weight_slot),
                                            float(grid_half_width), int(grid_steps), ptr(hu), ptr(hp), ptr(dp)))
     return hu, hp, dp
+
+
+def polish_peaks_weights(table, cands, weight_slots, n_zeros: int | None = None,
+                         grid_half_width: float = 2.5e-4, grid_steps: int = 40):
+    """polish_peaks_exact under several registered weight vectors at once: (h_unpol, h_pol,
+    ddy_pol), each of shape (len(weight_slots), P).  The exact (A, B) is built once in device
+    memory and read by every weight's polish (search/eval_tech1_600k.py:216-273)."""
+    vi, vf, d = _cands(cands)
+    P = vi.shape[0]
+    n = table.n if n_zeros is None else int(n_zeros)
+    slots = np.ascontiguousarray(weight_slots, dtype=np.int32)
+    W = slots.shape[0]
+    hu, hp, dp = np.empty((W, P)), np.empty((W, P)), np.empty((W, P))
+    check(_lib.lib().mb_polish_peaks_weights(table.handle, P, ptr(vi), ptr(vf), ptr(d), n, W, ptr(slots),
+                                             float(grid_half_width), int(grid_steps), ptr(hu), ptr(hp), ptr(dp)))
+    return hu, hp, dp

@@ -3,8 +3,9 @@
 search/eval_tech1_600k.py:216-273 (and eval_tech2_hdrop_600k.py, eval_sub35_candidates.py) score
 their candidates by compute_peak_AB over all N zeros followed by one polish_peaks_with_weights per
 weight vector (grid_half_width 2.5e-4, 40 steps): the P x N A/B matrices are built once and read
-five times.  Here each weight vector is registered with the table once and each polish is one
-mb_polish_peaks_exact call, which computes (A_j, B_j) from the exact phase on the fly:
+five times.  Here each weight vector is registered with the table once and all polishes are one
+mb_polish_peaks_weights call, which writes the exact-phase (A_j, B_j) of the candidates to device
+memory once and runs every weight's polish from it:
 
     table = k2.ZeroTable.from_data(data)
     cands = candidates_from_x(x, dy)                 # the drivers' x = floor(y 2^30) and dy
@@ -51,8 +52,7 @@ def score(table, cands, weights: dict[str, np.ndarray], grid_half_width: float =
           n_zeros: int | None = None) -> dict[str, tuple[np.ndarray, np.ndarray, np.ndarray]]:
     """name -> (h_unpol, h_pol, ddy_pol) of polish_peaks_with_weights for each weight vector
     (length table.n), over the first n_zeros zeros (all by default)."""
-    out = {}
-    for name, w in weights.items():
-        slot = table.add_weights(w)
-        out[name] = path1.polish_peaks_exact(table, cands, slot, n_zeros, grid_half_width, grid_steps)
-    return out
+    names = list(weights)
+    slots = [table.add_weights(weights[name]) for name in names]
+    hu, hp, dp = path1.polish_peaks_weights(table, cands, slots, n_zeros, grid_half_width, grid_steps)
+    return {name: (hu[i], hp[i], dp[i]) for i, name in enumerate(names)}

@@ -47,3 +47,35 @@ def test_score_matches_reference_evaluator(setup):
         assert np.max(np.abs(hu - hu0)) < 1e-12, name
         assert np.max(np.abs(hp - hp0)) < 1e-11, name
         assert np.max(np.abs(dp - dp0)) < 1e-9, name
+
+
+def test_weights_call_equals_single_weight_calls(setup):
+    """mb_polish_peaks_weights reads the exact A/B from a device matrix; each of its rows equals
+    the single-weight matrix-free call (the same A/B values, the same polish)."""
+    t, cd, table = setup
+    W = score.reference_weights(t.gamma)
+    slots = [table.add_weights(w) for w in W.values()]
+    hu, hp, dp = path1.polish_peaks_weights(table, cd, slots)
+    assert hu.shape == (len(W), cd.n)
+    for i, s in enumerate(slots):
+        gu, gp, gd = path1.polish_peaks_exact(table, cd, s)
+        np.testing.assert_allclose(hu[i], gu, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(hp[i], gp, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(dp[i], gd, rtol=0, atol=1e-15)
+    hz = path1.polish_peaks_weights(table, cd, slots[:2], n_zeros=0)     # no zeros: all sums are 0
+    assert np.all(hz[0] == 0.0) and np.all(hz[1] == 0.0)
+
+
+def test_weights_call_in_chunks(gpu):
+    """600,000 zeros: the 4 GiB matrix budget holds 447 peaks, so 460 candidates take two chunks."""
+    data = synth.make_table(600_000, seed=72)
+    cd = synth.make_candidates(460, seed=73)
+    cd.delta[:] = np.random.default_rng(73).uniform(-1e-4, 1e-4, cd.n)
+    with k2.ZeroTable.from_data(data) as table:
+        w = score.reference_weights(data.gamma)["jp"]
+        s = table.add_weights(w)
+        hu, hp, dp = path1.polish_peaks_weights(table, cd, [s])
+        gu, gp, gd = path1.polish_peaks_exact(table, cd, s)
+    np.testing.assert_allclose(hu[0], gu, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(hp[0], gp, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(dp[0], gd, rtol=0, atol=1e-15)
