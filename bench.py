@@ -747,8 +747,11 @@ def run_profile_extras():
     """One launch each of the kernels beside the tiers, at modest sizes (~0.5 GB on the device):
     the certified interval over all 2,325,572 zeros at the Peak2 point, the leaf screen (4,096
     leaves, 64/128/256 zeros), polish_peaks_with_weights matrix-free (32 candidates x 100,000
-    zeros) and the Taylor-moment polish matrix-free (256 candidates x 100,000 zeros)."""
-    from mertens_bound_b200 import hit_polish, k2, path1, synth
+    zeros), the Taylor-moment polish matrix-free (256 candidates x 100,000 zeros), then the hit
+    scans of 16 hits through the five ZeroData::polish stages, polish.py's 25,001-point grid over
+    the zeros below 74,000, and the five-weight scoring of 32 candidates from one exact A/B
+    matrix (100,000 zeros)."""
+    from mertens_bound_b200 import hit_polish, k2, path1, polish, score, synth
     big = synth.make_table(2_325_572, seed=1)
     with k2.ZeroTable.from_data(big) as tb:
         k2.k2_certified(tb, synth.peak2_candidate(), 1.5e-10, 1.3e6, v_rad=2.0 ** -64)
@@ -760,6 +763,9 @@ def run_profile_extras():
         slot = t.add_weights(np.exp(-3e-9 * d.gamma * d.gamma))
         path1.polish_peaks_exact(t, c.subset(np.arange(32)), slot)
         path1.fast_polish_exact(t, c.subset(np.arange(256)), slot)
+        hit_polish.polish_hits(t, pts[:16], thresholds=(None, None, None))
+        polish.scan(t, synth.PEAK2_STR, 0.25, 2e-5)
+        score.score(t, c.subset(np.arange(32)), score.reference_weights(d.gamma))
     print(json.dumps({"profile_case": "extras", "screen_hits": int(len(r.hits))}), flush=True)
 
 

@@ -130,8 +130,10 @@ k2_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, u
     }
 }
 
-// Small grids over many base points (the hit polish of the enumerators): one CTA per base point,
-// each thread HIT_ZPT zeros per round.  Per zero: the exact phase at the grid's first point and
+// Small grids over many base points (the hit polish of the enumerators): n_split CTAs per base
+// point, each over a contiguous share of the zeros (so a few hits still fill the GPU), each thread
+// HIT_ZPT zeros per round; the shares' sums go to partial[(p n_split + s) n_m + m] and
+// hit_reduce_kernel adds them in split order.  Per zero: the exact phase at the grid's first point and
 // the exact increment per step; every HIT_MB points an exact anchor (FP64 sine/cosine of the
 // 128-bit phase, times the amplitude), rotated to the points in between by powers of the
 // increment's (cos, sin).  A block of HIT_MB points is summed over the thread's zeros, then over
@@ -145,9 +147,10 @@ static_assert(HIT_MB == 16, "add_rotations16 and the anchor step (increment << 4
 
 __global__ void __launch_bounds__(HIT_THREADS)
 k2_hit_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t si, uint64_t sf, int64_t m0, int n_m,
-                   int64_t n_use, double k, double *out_h) {
+                   int64_t n_use, double k, int n_split, double *partial) {
     extern __shared__ double acc[];            // [HIT_THREADS / 32][n_m]
-    const int p = blockIdx.x;
+    const int64_t p = blockIdx.x / n_split;
+    const int split = blockIdx.x - (int)(p * n_split);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < (HIT_THREADS / 32) * n_m; i += HIT_THREADS) acc[i] = 0.0;
     __syncthreads();
@@ -155,7 +158,8 @@ k2_hit_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t s
     const uint32_t mabs = (uint32_t)(m0 < 0 ? -m0 : m0);
     constexpr int PER_ROUND = HIT_THREADS * HIT_ZPT;
     const int64_t rounds = (n_use + PER_ROUND - 1) / PER_ROUND;
-    for (int64_t r = 0; r < rounds; ++r) {
+    const int64_t r_end = rounds * (split + 1) / n_split;
+    for (int64_t r = rounds * split / n_split; r < r_end; ++r) {
         uint64_t xlo[HIT_ZPT], xhi[HIT_ZPT], dlo[HIT_ZPT], dhi[HIT_ZPT];
         double a[HIT_ZPT], rc[HIT_ZPT][4], rs[HIT_ZPT][4];
 #pragma unroll
@@ -215,8 +219,18 @@ k2_hit_scan_kernel(TabView t, const uint64_t *vi, const uint64_t *vf, uint64_t s
     for (int m = threadIdx.x; m < n_m; m += HIT_THREADS) {
         double s = 0.0;
         for (int w = 0; w < HIT_THREADS / 32; ++w) s += acc[w * n_m + m];
-        out_h[(int64_t)p * n_m + m] = s;
+        partial[(int64_t)blockIdx.x * n_m + m] = s;
     }
+}
+
+__global__ void hit_reduce_kernel(const double *partial, int64_t P, int n_split, int n_m, double *h) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= P * n_m) return;
+    const int64_t p = idx / n_m;
+    const int m = (int)(idx - p * n_m);
+    double s = 0.0;
+    for (int c = 0; c < n_split; ++c) s += partial[(p * n_split + c) * n_m + m];
+    h[idx] = s;
 }
 
 __global__ void scan_reduce_kernel(const double *partial, int P, int n_chunk, int n_m, double *h) {
@@ -297,11 +311,20 @@ extern "C" int mb_hit_scan(mb_table *h, int64_t P, const uint64_t *v_int, const 
     double *d_h = (double *)(base + ((2 * cb + 255) & ~(size_t)255));
     MB_CUDA(cudaMemcpyAsync(d_vi, v_int, cb, cudaMemcpyHostToDevice, t.stream));
     MB_CUDA(cudaMemcpyAsync(d_vf, v_frac, cb, cudaMemcpyHostToDevice, t.stream));
+    // splits per hit: about 8 CTAs per SM in all, each split at least two rounds of zeros
+    int sms = 148;
+    MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, t.device));
+    const int64_t rounds = (n_use + HIT_THREADS * HIT_ZPT - 1) / (HIT_THREADS * HIT_ZPT);
+    const int n_split = (int)std::max<int64_t>(1, std::min<int64_t>((8 * sms + P - 1) / P, rounds / 2));
+    MB_TRY(t.work.ensure((size_t)P * n_split * n_m * sizeof(double)));
+    double *partial = (double *)t.work.p;
     const size_t smem = (size_t)(HIT_THREADS / 32) * n_m * sizeof(double);
     if (smem > 48 * 1024)
         MB_CUDA(cudaFuncSetAttribute(k2_hit_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k2_hit_scan_kernel<<<(unsigned)P, HIT_THREADS, smem, t.stream>>>(view(t), d_vi, d_vf, step_int, step_frac, m0,
-                                                                      (int)n_m, n_use, k, d_h);
+    k2_hit_scan_kernel<<<(unsigned)(P * n_split), HIT_THREADS, smem, t.stream>>>(
+        view(t), d_vi, d_vf, step_int, step_frac, m0, (int)n_m, n_use, k, n_split, partial);
+    MB_CUDA(cudaGetLastError());
+    hit_reduce_kernel<<<(unsigned)((P * n_m + 255) / 256), 256, 0, t.stream>>>(partial, P, n_split, (int)n_m, d_h);
     MB_CUDA(cudaGetLastError());
     MB_CUDA(cudaMemcpyAsync(out_h, d_h, hb, cudaMemcpyDeviceToHost, t.stream));
     MB_CUDA(cudaStreamSynchronize(t.stream));
