@@ -5,8 +5,9 @@
 //   heavy tier  j <  n_h : 64-bit phase (3 IMAD.lo + 4 DFMA + 4 FFMA, error ~2^-48 turn), sin/cos
 //                          from a 1024-entry table rotated by short FP64 polynomials, FP64
 //                          accumulation.                                  -> k2_heavy_kernel
-//   light tier  j >= n_h : 32-bit phase (3 IMAD.lo + 4 DFMA in two chains), MUFU sin/cos of
-//                          the reduced phase, FP32 accumulation flushed every LIGHT_FLUSH terms
+//   light tier  j >= n_h : 32-bit phase (3 IMAD.lo + 4 DFMA in two chains; 2 IMAD.lo + 3 DFMA
+//                          when every zero has gamma < 3.29e6, light_phase32_fused), MUFU sin/cos
+//                          of the reduced phase, FP32 accumulation flushed every LIGHT_FLUSH terms
 //                          into FP64 partials.                           -> k2_light_kernel
 // The heavy kernel is persistent with two CTAs per SM (FP64-pipe bound); the light kernel is
 // launched concurrently on a second stream with one CTA per work item and takes each SM as the
@@ -22,6 +23,7 @@
 // arg(c)/2pi (psi) is added to the phase, so each term is a cos(2pi u) with a = 2|c| w.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "k2_common.cuh"
@@ -36,6 +38,14 @@ struct __align__(16) ZLight {   // 64 B
     uint32_t b0, b1, gi, psi32;  // psi32 = round(psi 2^32) + 2 (centres the truncation bias)
     double b0s, c1s, gis, b1s;   // limb 2^-32 (exact)
     float a, b, d, pad;          // a = 2|c|w, b = -a gamma, d = -a gamma^2
+};
+
+struct __align__(16) ZLightF {  // 48 B: the light record of light_phase32_fused
+    uint32_t b0, b1, psi32;      // as in ZLight, psi32 = round(psi 2^32) + 1
+    float a;                     // a = 2|c|w
+    double b0s, c1s;             // limb 2^-32 (exact)
+    double gh;                   // gI 2^32 + b1 (exact for gI < 2^19)
+    float b, d;                  // b = -a gamma, d = -a gamma^2
 };
 
 struct __align__(16) ZHeavy {   // 96 B
@@ -53,21 +63,28 @@ constexpr int LIGHT_FLUSH = 16;
 // shared memory: the staged tile, reused after the tile loop for the cross-warp reduction
 constexpr int FAST_SMEM = 24576;
 static_assert(FAST_SMEM >= LIGHT_TILE * sizeof(ZLight), "light tile");
+static_assert(sizeof(ZLightF) == 48, "fused light record");
 static_assert(FAST_SMEM >= HEAVY_TILE * sizeof(ZHeavy), "heavy tile");
 static_assert(FAST_SMEM >= FAST_THREADS * 4 * 3 * sizeof(double), "reduction buffer");
 
-template <int CPT>
-MB_DEV void light_tile(const ZLight *tile, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
+template <int CPT, bool FUSED>
+MB_DEV void light_tile(const void *tile_v, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
                        double (&sum)[CPT][3]) {
+    using Rec = typename std::conditional<FUSED, ZLightF, ZLight>::type;
+    const Rec *tile = static_cast<const Rec *>(tile_v);
     float acc[CPT][3];
 #pragma unroll
     for (int i = 0; i < CPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
     int cnt = 0;
     for (int jj = zl; jj < nt; jj += ZL) {
-        const ZLight z = tile[jj];
+        const Rec z = tile[jj];
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
-            int32_t u = (int32_t)light_phase32(cr[i], z.b0, z.b1, z.gi, z.b0s, z.c1s, z.gis, z.b1s, z.psi32);
+            int32_t u;
+            if constexpr (FUSED)
+                u = (int32_t)light_phase32_fused(cr[i], z.b0, z.b1, z.b0s, z.c1s, z.gh, z.psi32);
+            else
+                u = (int32_t)light_phase32(cr[i], z.b0, z.b1, z.gi, z.b0s, z.c1s, z.gis, z.b1s, z.psi32);
             float th = (float)u * 1.4629180792671596e-09f;      // 2pi 2^-32
             float s = __sinf(th), co = __cosf(th);
             acc[i][0] = fmaf(z.a, co, acc[i][0]);
@@ -148,6 +165,22 @@ MB_DEV void stage_light(const TabView &t, int64_t j, double k, const double *w, 
     r.pad = 0.f;
 }
 
+MB_DEV void stage_light(const TabView &t, int64_t j, double k, const double *w, ZLightF &r) {
+    double g = t.gamma[j];
+    double a = 2.0 * t.alpha[j] * (w ? w[j] : exp(-k * g * g));
+    uint32_t b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j], c1 = t.g1[j];
+    r.b0 = b0; r.b1 = b1;
+    // + 1 centres the fused phase's truncation (dropped products in [0, 3) units): error within
+    // +-2.4 units of 2^-32 turn
+    r.psi32 = (uint32_t)((t.psi[j] + 0x80000000ull) >> 32) + 1u;
+    r.b0s = u32_to_f64(b0) * TWO_M32;
+    r.c1s = u32_to_f64(c1) * TWO_M32;
+    r.gh = fma(u32_to_f64(gi), 4294967296.0, u32_to_f64(b1));
+    r.a = (float)a;
+    r.b = (float)(-a * g);
+    r.d = (float)(-a * g * g);
+}
+
 MB_DEV void stage_heavy(const TabView &t, int64_t j, double k, const double *w, ZHeavy &r) {
     double g = t.gamma[j];
     double a = 2.0 * t.alpha[j] * (w ? w[j] : exp(-k * g * g));
@@ -202,9 +235,10 @@ MB_DEV void finish_item(const FastItem &it, const FastGroup &gr, double (&res)[C
     }
 }
 
-template <int CPT>
+template <int CPT, bool FUSED>
 MB_DEV void light_item(const FastItem &it, const FastGroup &gr, const TabView &t, const CandView &c,
                        double *partial, unsigned char *smem) {
+    using Rec = typename std::conditional<FUSED, ZLightF, ZLight>::type;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nzw = it.nzw;
     const int cgroup = warp / nzw, zw = warp - cgroup * nzw;
@@ -213,7 +247,7 @@ MB_DEV void light_item(const FastItem &it, const FastGroup &gr, const TabView &t
     CandRegs cr[CPT];
 #pragma unroll
     for (int i = 0; i < CPT; ++i) cr[i] = cand_regs(c, cbase + i, cbase + i < cend);
-    ZLight *tile = reinterpret_cast<ZLight *>(smem);
+    Rec *tile = reinterpret_cast<Rec *>(smem);
     double res[CPT][3];
 #pragma unroll
     for (int i = 0; i < CPT; ++i)
@@ -224,7 +258,7 @@ MB_DEV void light_item(const FastItem &it, const FastGroup &gr, const TabView &t
         int64_t j = tb + threadIdx.x;
         if (threadIdx.x < LIGHT_TILE && j < it.z1) stage_light(t, j, gr.k, gr.w, tile[threadIdx.x]);
         __syncthreads();
-        light_tile<CPT>(tile, (int)min((int64_t)LIGHT_TILE, it.z1 - tb), zw, nzw, cr, res);
+        light_tile<CPT, FUSED>(tile, (int)min((int64_t)LIGHT_TILE, it.z1 - tb), zw, nzw, cr, res);
     }
     finish_item<CPT>(it, gr, res, warp, lane, zw, cbase, cend, partial, smem);
 }
@@ -279,12 +313,12 @@ k2_heavy_kernel(TabView t, CandView c, const FastItem *items, int n_items, const
 }
 
 // Light tier: one CTA per item.  MINB sets the register budget (65536 / (256 MINB)).
-template <int CPT, int MINB>
+template <int CPT, int MINB, bool FUSED>
 __global__ void __launch_bounds__(FAST_THREADS, MINB)
 k2_light_kernel(TabView t, CandView c, const FastItem *items, const FastGroup *groups, double *partial) {
     __shared__ __align__(16) unsigned char smem[FAST_SMEM];
     const FastItem it = items[blockIdx.x];
-    light_item<CPT>(it, groups[it.group], t, c, partial, smem);
+    light_item<CPT, FUSED>(it, groups[it.group], t, c, partial, smem);
 }
 
 // One warp per candidate: lane l sums chunks l, l+32, ... of the candidate's group, then a fixed
@@ -322,10 +356,18 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
     if (pd.n_light == 0) return MB_OK;
     dim3 grid((unsigned)pd.n_light);
     const FastItem *li = pd.items + pd.n_heavy;
-    switch (pd.light_cpt) {
-        case 2: k2_light_kernel<2, 4><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
-        case 3: k2_light_kernel<3, 3><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
-        default: k2_light_kernel<4, 2><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+    if (pd.fused_phase) {
+        switch (pd.light_cpt) {
+            case 2: k2_light_kernel<2, 4, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+            case 3: k2_light_kernel<3, 3, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+            default: k2_light_kernel<4, 2, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+        }
+    } else {
+        switch (pd.light_cpt) {
+            case 2: k2_light_kernel<2, 4, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+            case 3: k2_light_kernel<3, 3, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+            default: k2_light_kernel<4, 2, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, li, pd.groups, pd.partial); break;
+        }
     }
     MB_CUDA(cudaGetLastError());
     return MB_OK;

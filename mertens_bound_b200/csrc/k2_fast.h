@@ -39,6 +39,8 @@ struct FastPlanDev {
     FastGroup *groups = nullptr;
     int n_heavy = 0, n_light = 0, n_groups = 0;
     int light_cpt = 4;          // candidates per thread of the light kernel: 2, 3 or 4
+    bool fused_phase = false;   // light tier on light_phase32_fused: every zero has gamma below
+                                // FUSED_PHASE_GAMMA, so G's integer part is below 2^19
     unsigned heavy_grid = 0;
     int *counter = nullptr;
     double *partial = nullptr;
@@ -53,6 +55,8 @@ struct FastPlanDev {
 //   heavy: phase 2^-47 turn, table + polynomial 3e-15, FP64 roundings  ->  2e-13 (kept loose:
 //          the heavy amplitude sum is O(1), so this share of the bound is negligible)
 constexpr double EPS_LIGHT = 2.2e-6;
+// 2 pi (2^19 - 1): below it G = gamma / 2pi has an integer part below 2^19
+constexpr double FUSED_PHASE_GAMMA = 6.283185307179586 * 524287.0;
 constexpr double EPS_HEAVY = 2.0e-13;
 
 int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,

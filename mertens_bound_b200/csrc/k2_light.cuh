@@ -23,6 +23,7 @@ constexpr double TWO_M96 = 1.2621774483536189e-29;
 struct CandRegs {
     uint32_t a0, a1, d1, d0;
     double A0, A1, D0, D1;      // exact doubles of the limbs a0, a1, d0, d1
+    double VF;                  // v_frac 2^-64 rounded to double (light_phase32_fused)
 };
 
 MB_DEV CandRegs cand_regs_of(Cand64 v) {
@@ -35,6 +36,7 @@ MB_DEV CandRegs cand_regs_of(Cand64 v) {
     r.A1 = u32_to_f64(r.a1);
     r.D0 = u32_to_f64((uint32_t)v.vf);
     r.D1 = u32_to_f64(r.d1);
+    r.VF = __ull2double_rn(v.vf) * TWO_M64;
     return r;
 }
 
@@ -53,6 +55,20 @@ MB_DEV uint32_t light_phase32(const CandRegs &c, uint32_t b0, uint32_t b1, uint3
     const uint32_t lo32 = c.a1 * b0 + c.a0 * b1 + c.d1 * gi + add;
     const double R1 = fma(c.A0, b0s, fma(c.A1, c1s, MAGIC));
     const double R2 = fma(c.D0, gis, fma(c.D1, b1s, MAGIC));
+    return lo32 + (uint32_t)__double2loint(R1) + (uint32_t)__double2loint(R2);
+}
+
+// The same phase when G's integer part gI is below 2^19 (gamma < 3.29e6): the whole fraction part
+// of v enters through one product,
+//   v_frac 2^-64 (gI + b1 2^-32) 2^32 = VF gh,   gh = gI 2^32 + b1 (exact, < 2^51),
+// rounded to an integer on top of 1.5 2^52 (VF carries v_frac to 53 bits: <= 2^-3 unit of error),
+// so d1 gI leaves the integer sum and d0 gI, d1 b1 leave the FP64 one: 2 IMAD.lo + 3 DFMA.
+// Dropped: a1 c0 2^-64, a0 c1 2^-64 and v_frac b0 2^-96, below 3 units in all.
+MB_DEV uint32_t light_phase32_fused(const CandRegs &c, uint32_t b0, uint32_t b1, double b0s, double c1s, double gh,
+                                    uint32_t add) {
+    const uint32_t lo32 = c.a1 * b0 + c.a0 * b1 + add;
+    const double R1 = fma(c.A0, b0s, fma(c.A1, c1s, MAGIC));
+    const double R2 = fma(c.VF, gh, MAGIC);
     return lo32 + (uint32_t)__double2loint(R1) + (uint32_t)__double2loint(R2);
 }
 

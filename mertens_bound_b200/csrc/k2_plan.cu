@@ -238,6 +238,7 @@ int upload(mb_plan *p) {
     p->dev.n_light = (int)p->items.size() - p->n_heavy_items;
     p->dev.n_groups = (int)p->groups.size();
     p->dev.light_cpt = p->light_cpt;
+    p->dev.fused_phase = p->table->h_gamma.empty() || p->table->h_gamma.back() < FUSED_PHASE_GAMMA;
     unsigned hg = 148;
     MB_TRY(heavy_grid_size(p->table->device, &hg));
     p->dev.heavy_grid = std::min<unsigned>(hg, (unsigned)std::max(1, p->n_heavy_items));
