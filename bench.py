@@ -43,13 +43,14 @@ T0, K_GAUSS, P_PER_GPU, TOL = 3e5, 3e-9, 4096, 1e-10
 WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 candidates v~3.5e18 "
             "per GPU, k=3e-9, K2 + dK2/ddelta + dK2/dk per candidate, a-priori |err| <= 1e-10")
 # Warp instructions per warp of zero-terms (= thread instructions per zero-term) of the two
-# tier kernels -- the light tier for each candidates-per-thread setting -- and their DRAM bytes
-# per launch on this workload, from the ncu capture of `bench.py --profile-case search`
-# summarised in profiles/k2_light_kernel_search_scoring.md.
-LIGHT_INST_PER_TERM = {2: 23.40, 3: 25.62, 4: 20.03}
-HEAVY_INST_PER_TERM = 41.09
-LIGHT_DRAM_BYTES = {2: 16487680, 3: 16466176, 4: 16446464}
-HEAVY_DRAM_BYTES = 2781952
+# tier kernels -- the light tier (its one-FMA fraction product, as every zero here lies below
+# gamma = 3.29e6) for each candidates-per-thread setting -- and their DRAM bytes per launch on this
+# workload, from the ncu capture of `bench.py --profile-case search` summarised in
+# profiles/k2_light_kernel_search_scoring.md.
+LIGHT_INST_PER_TERM = {2: 21.39, 3: 21.50, 4: 17.97}
+HEAVY_INST_PER_TERM = 41.04
+LIGHT_DRAM_BYTES = {2: 16486656, 3: 16500480, 4: 16445952}
+HEAVY_DRAM_BYTES = 2775552
 REF_SAMPLE_CANDS = 64
 
 

@@ -15,16 +15,24 @@ P = 1 << 18
 
 
 def one_zero(j):
+    """Zero j of the synthetic table, or (j a float) one zero at gamma = j with random low bits of G
+    and the coefficient of the table's last zero below 3e5."""
+    if isinstance(j, float):
+        t = synth.make_table_below(3e5, seed=1)
+        G3 = synth.fixed_from_double(np.array([j / (2.0 * math.pi)]), np.random.default_rng(11))
+        return synth.ZeroTableData(G3, synth.gamma_from_fixed(G3), t.c_re[-1:].copy(), t.c_im[-1:].copy(), t.seed)
     t = synth.make_table_below(3e5, seed=1) if j > 0 else synth.make_table(1, seed=5)
     return synth.ZeroTableData(t.G3[j:j + 1].copy(), t.gamma[j:j + 1].copy(), t.c_re[j:j + 1].copy(),
                                t.c_im[j:j + 1].copy(), t.seed)
 
 
-@pytest.mark.parametrize("j", [0, 400_000])
+# 3.2e6: the light tier's one-FMA fraction product at an integer part of G near its 2^19 limit;
+# 5e6: above the limit, the split light phase
+@pytest.mark.parametrize("j", [0, 400_000, 3.2e6, 5.0e6])
 @pytest.mark.parametrize("tier,tol", [("light", 1.0), ("heavy", 1e-30)])
 def test_per_term_error_within_bound(gpu, oracle, j, tier, tol):
     data = one_zero(j)
-    cd = synth.make_candidates(P, seed=17 + j)
+    cd = synth.make_candidates(P, seed=17 + int(j))
     ohi, _ = oracle.k2(cd, data, 0.0, 1)
     with k2.ZeroTable.from_data(data) as t, k2.Plan(t, [P], [0.0], [math.inf], tol=tol) as plan:
         gi = plan.group_info(0)
