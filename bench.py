@@ -629,12 +629,20 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
         cl = synth.make_candidates(1 << 20, seed=7)
         pts = np.stack([cl.v_int, cl.v_frac], axis=1)
         hit_polish.screen_leaves(t6, pts[:4096])
-        t0 = time.perf_counter()
-        r = hit_polish.screen_leaves(t6, pts, max_hits=1 << 20)
-        sc_s = time.perf_counter() - t0
+
+        def wall(fn, reps=3):
+            """Median wall seconds of fn() over reps calls, and its last result."""
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                res = fn()
+                ts.append(time.perf_counter() - t0)
+            return statistics.median(ts), res
+
+        sc_s, r = wall(lambda: hit_polish.screen_leaves(t6, pts, max_hits=1 << 20))
         out["enumerator_screen"] = {"leaves": len(pts), "seconds": sc_s, "leaves_per_s": len(pts) / sc_s,
                                     "hits": int(len(r.hits)), "stages": "64/128/256 zeros, 0.78/0.855/0.892",
-                                    "note": "host-pointer call: includes the H2D of 16 MB of leaves"}
+                                    "note": "host-pointer call: includes the H2D of 16 MB of leaves; median of 3 calls"}
         reft = None
         if cpu_baseline:
             try:
@@ -646,18 +654,14 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
                 out["enumerator_screen"]["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
         hits = pts[:256]
         hit_polish.polish_hits(t6, hits[:8])
-        t0 = time.perf_counter()
-        hr = hit_polish.polish_hits(t6, hits, thresholds=(None, None, None))
-        hp_s = time.perf_counter() - t0
+        hp_s, hr = wall(lambda: hit_polish.polish_hits(t6, hits, thresholds=(None, None, None)))
         out["hit_polish"] = {"hits": 256, "zeros": d600.n, "seconds": hp_s, "hits_per_s": 256 / hp_s,
                              "stages_run": int(hr.stage.max()) + 1, "thresholds": "none (every hit runs all stages)"}
         if reft is not None:
             out["hit_polish"]["cpu_baseline"] = hit_polish_cpu(d600, hits, reft)
         n74 = t6.count_below(polish.POLISH_T)
         polish.scan(t6, synth.PEAK2_STR, 0.001, 2e-5)
-        t0 = time.perf_counter()
-        best, y_best, m_best = polish.scan(t6, synth.PEAK2_STR, 0.25, 2e-5)
-        ps_s = time.perf_counter() - t0
+        ps_s, (best, y_best, m_best) = wall(lambda: polish.scan(t6, synth.PEAK2_STR, 0.25, 2e-5))
         out["polish_scan"] = {"points": 25001, "zeros": n74, "seconds": ps_s,
                               "point_zero_terms_per_s": 25001 * n74 / ps_s, "best_abs_h": abs(best)}
         if cpu_baseline:
