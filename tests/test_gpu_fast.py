@@ -201,3 +201,27 @@ def test_shards_with_skip_and_weights(gpu, oracle):
         ohi, _ = oracle.k2(cd.subset(np.arange(32 * g, 32 * g + 32)), data, k, n, weights=w)
         assert np.max(np.abs(full[sl, 0] - ohi[:, 0])) <= bounds[g]["err_bound"]
         assert np.max(np.abs(tot[sl, 0] - full[sl, 0])) <= 2 * bounds[g]["err_bound"]
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-7, 1e-8])
+def test_high_gamma_table(gpu, small_table, oracle, tol):
+    """A table of 3,000 zeros above gamma = 5e6: G's integer part exceeds 2^19, so the light tier
+    takes its split fraction product (the one-FMA form needs gamma < 3.29e6).  Raw weights (k = 0)
+    and the coefficients of zeros 7,000-9,999 of the small table: tol 1e-6 puts every zero in the
+    light tier, 1e-7 about two thirds in the heavy one, 1e-8 nearly all."""
+    rng = np.random.default_rng(91)
+    gam = 5.0e6 + np.cumsum(rng.uniform(0.2, 0.72, 3000))
+    G3 = synth.fixed_from_double(gam / (2.0 * math.pi), rng)
+    data = synth.ZeroTableData(G3, synth.gamma_from_fixed(G3), small_table.c_re[7000:10000].copy(),
+                               small_table.c_im[7000:10000].copy(), small_table.seed)
+    cd = synth.make_candidates(64, seed=92)
+    ohi, _ = oracle.k2(cd, data, 0.0, data.n)
+    with k2.ZeroTable.from_data(data) as t:
+        val, dd, dk, eb = k2.k2_fast(t, cd, 0.0, tol=tol)
+        with k2.Plan(t, [64], [0.0], [math.inf], tol=tol) as plan:
+            gi = plan.group_info(0)
+    assert gi["n_heavy"] < data.n and (gi["n_heavy"] > 0) == (tol < 1e-6)
+    assert eb <= tol
+    assert np.max(np.abs(val - ohi[:, 0])) <= eb
+    assert np.max(np.abs(dd - ohi[:, 1])) <= gi["err_bound_dd"]
+    assert np.max(np.abs(dk - ohi[:, 2])) <= gi["err_bound_dk"]
