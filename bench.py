@@ -592,12 +592,16 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
     c6.delta[:] = np.random.default_rng(6).uniform(-1e-4, 1e-4, 256)
     W = score.reference_weights(d600.gamma)
     with k2.ZeroTable.from_data(d600, device=dev.index) as t6:
-        score.score(t6, c6.subset(np.arange(8)), W)                       # registers the vectors
-        t0 = time.perf_counter()
-        res = score.score(t6, c6, W)
-        gpu_s = time.perf_counter() - t0
+        slots = score.register(t6, W)                                    # once per table
+        score.score(t6, c6.subset(np.arange(8)), slots)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            res = score.score(t6, c6, slots)
+            ts.append(time.perf_counter() - t0)
+        gpu_s = statistics.median(ts)
     ds = {"candidates": 256, "zeros": 600_000, "weights": list(W), "grid": "2.5e-4 / 40 steps",
-          "seconds": gpu_s, "candidates_per_s": 256 / gpu_s,
+          "seconds": gpu_s, "candidates_per_s": 256 / gpu_s, "timing": "median of 3 calls, slots registered once",
           "best_abs_h_pol": float(max(np.max(np.abs(v[1])) for v in res.values()))}
     if cpu_baseline:
         try:

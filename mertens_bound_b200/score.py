@@ -8,8 +8,9 @@ mb_polish_peaks_weights call, which writes the exact-phase (A_j, B_j) of the can
 memory once and runs every weight's polish from it:
 
     table = k2.ZeroTable.from_data(data)
+    slots = register(table, reference_weights(data.gamma))   # once per table
     cands = candidates_from_x(x, dy)                 # the drivers' x = floor(y 2^30) and dy
-    res = score(table, cands, reference_weights(data.gamma))
+    res = score(table, cands, slots)
     h_unpol, h_pol, ddy_pol = res["jp"]
 """
 from __future__ import annotations
@@ -48,11 +49,20 @@ def candidates_from_x(x, dy=None) -> synth.Candidates:
     return synth.Candidates(vi, vf, d.copy())
 
 
-def score(table, cands, weights: dict[str, np.ndarray], grid_half_width: float = 2.5e-4, grid_steps: int = 40,
+def register(table, weights: dict[str, np.ndarray]) -> dict[str, int]:
+    """name -> slot of each weight vector (length table.n) registered with the table; a driver
+    registers its vectors once and passes the slots to every score() call."""
+    return {name: table.add_weights(w) for name, w in weights.items()}
+
+
+def score(table, cands, weights: dict, grid_half_width: float = 2.5e-4, grid_steps: int = 40,
           n_zeros: int | None = None) -> dict[str, tuple[np.ndarray, np.ndarray, np.ndarray]]:
-    """name -> (h_unpol, h_pol, ddy_pol) of polish_peaks_with_weights for each weight vector
-    (length table.n), over the first n_zeros zeros (all by default)."""
+    """name -> (h_unpol, h_pol, ddy_pol) of polish_peaks_with_weights for each weight vector, over
+    the first n_zeros zeros (all by default).  Each value of `weights` is a slot from register()
+    (or ZeroTable.add_weights), or a weight vector of length table.n, which is registered first
+    (hashing it to find a slot registered before: milliseconds per vector, so pass slots in a
+    loop)."""
     names = list(weights)
-    slots = [table.add_weights(weights[name]) for name in names]
+    slots = [w if isinstance(w, (int, np.integer)) else table.add_weights(w) for w in weights.values()]
     hu, hp, dp = path1.polish_peaks_weights(table, cands, slots, n_zeros, grid_half_width, grid_steps)
     return {name: (hu[i], hp[i], dp[i]) for i, name in enumerate(names)}

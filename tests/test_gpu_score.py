@@ -32,6 +32,10 @@ def test_score_matches_matrix_path(setup):
         np.testing.assert_allclose(gd, dp, rtol=0, atol=1e-12, err_msg=name)
     again = score.score(table, cd, W)              # registered vectors are reused
     assert all(np.array_equal(again[n][1], res[n][1]) for n in W)
+    slots = score.register(table, W)               # the same slots, passed directly
+    assert slots == {n: table.add_weights(w) for n, w in W.items()}
+    by_slot = score.score(table, cd, slots)
+    assert all(np.array_equal(by_slot[n][1], res[n][1]) for n in W)
 
 
 @pytest.mark.skipif(not RefLib.available(), reason="reference evaluator not built")
