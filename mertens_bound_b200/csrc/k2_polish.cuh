@@ -60,6 +60,10 @@ struct Team {
 };
 
 struct ABMatrix {
+    // zeros per iteration of the polish loops: the passes over a matrix are bound by global-load
+    // latency, so each iteration issues the loads of ZPI zeros before computing any of them
+    // (2: -20 % time at 64 registers; 3 spills, 4 takes 76 registers and is slower)
+    static constexpr int ZPI = 2;
     const double *A, *B;
     int64_t ld;
     struct Peak {
@@ -85,6 +89,7 @@ MB_DEV void two_sum(double a, double b, double &s, double &e) {
 //   part.  The angle error is below 2pi (|delta| 2^-52 + 2^-100) rad, so A and B carry the FP64
 //   rounding of sincospi and of 2 (c_re cos - c_im sin) only.  Requires |delta| <= 2^16.
 struct ABExact {
+    static constexpr int ZPI = 1;   // compute bound: one zero per iteration (more would spill)
     TabView t;
     const uint64_t *vi, *vf;
     const double *delta;   // may be null
@@ -140,12 +145,28 @@ struct ABExact {
 template <class Src>
 __device__ double polish_h(const Src &src, const typename Src::Peak &pk, int64_t n, const double *gamma,
                            const double *w, double ddy, Team &tm) {
+    constexpr int Z = Src::ZPI;
     double h = 0.0;
-    for (int64_t i = tm.first; i < n; i += POLISH_STRIDE) {
-        double a, b, sn, cs;
-        src.at(pk, i, a, b);
-        sincos(gamma[i] * ddy, &sn, &cs);
-        h += w[i] * (a * cs - b * sn);
+    for (int64_t i = tm.first; i < n; i += Z * POLISH_STRIDE) {
+        double a[Z], b[Z], g[Z], wv[Z];
+#pragma unroll
+        for (int z = 0; z < Z; ++z) {
+            const int64_t iz = i + z * POLISH_STRIDE;
+            a[z] = b[z] = g[z] = wv[z] = 0.0;
+            if (z == 0 || iz < n) {
+                src.at(pk, iz, a[z], b[z]);
+                g[z] = gamma[iz];
+                wv[z] = w[iz];
+            }
+        }
+        // the terms in zero order, as with one zero per iteration
+#pragma unroll
+        for (int z = 0; z < Z; ++z) {
+            if (z > 0 && i + z * POLISH_STRIDE >= n) break;
+            double sn, cs;
+            sincos(g[z] * ddy, &sn, &cs);
+            h += wv[z] * (a[z] * cs - b[z] * sn);
+        }
     }
     return tm.sum(h);
 }
@@ -158,16 +179,30 @@ __device__ double polish_newton(const Src &src, const typename Src::Peak &pk, in
                                 const double *w, double ddy, int iters, double clamp, double step_tol,
                                 Team &tm) {
     for (int it = 0; it < iters; ++it) {
+        constexpr int Z = Src::ZPI;
         double fp = 0.0, fpp = 0.0;
-        for (int64_t i = tm.first; i < n; i += POLISH_STRIDE) {
-            const double g = gamma[i];
-            double a, b, sn, cs;
-            src.at(pk, i, a, b);
-            sincos(g * ddy, &sn, &cs);
-            const double val = a * cs - b * sn;
-            const double dval = g * (-a * sn - b * cs);
-            fp += w[i] * dval;
-            fpp += w[i] * (-(g * g) * val);
+        for (int64_t i = tm.first; i < n; i += Z * POLISH_STRIDE) {
+            double a[Z], b[Z], g[Z], wv[Z];
+#pragma unroll
+            for (int z = 0; z < Z; ++z) {
+                const int64_t iz = i + z * POLISH_STRIDE;
+                a[z] = b[z] = g[z] = wv[z] = 0.0;
+                if (z == 0 || iz < n) {
+                    src.at(pk, iz, a[z], b[z]);
+                    g[z] = gamma[iz];
+                    wv[z] = w[iz];
+                }
+            }
+#pragma unroll
+            for (int z = 0; z < Z; ++z) {
+                if (z > 0 && i + z * POLISH_STRIDE >= n) break;
+                double sn, cs;
+                sincos(g[z] * ddy, &sn, &cs);
+                const double val = a[z] * cs - b[z] * sn;
+                const double dval = g[z] * (-a[z] * sn - b[z] * cs);
+                fp += wv[z] * dval;
+                fpp += wv[z] * (-(g[z] * g[z]) * val);
+            }
         }
         fp = tm.sum(fp);
         fpp = tm.sum(fpp);
@@ -231,11 +266,23 @@ __global__ void __cluster_dims__(POLISH_CLUSTER, 1, 1) __launch_bounds__(POLISH_
             a.ddy_pol[p] = better ? ddy : 0.0;
         }
     } else {
+        constexpr int Z = Src::ZPI;
         double s = 0.0;
-        for (int64_t i = tm.first; i < n; i += POLISH_STRIDE) {
-            double x, y;
-            src.at(pk, i, x, y);
-            s += a.w[i] * x;
+        for (int64_t i = tm.first; i < n; i += Z * POLISH_STRIDE) {
+            double x[Z], wv[Z];
+#pragma unroll
+            for (int z = 0; z < Z; ++z) {
+                const int64_t iz = i + z * POLISH_STRIDE;
+                x[z] = wv[z] = 0.0;
+                if (z == 0 || iz < n) {
+                    double y;
+                    src.at(pk, iz, x[z], y);
+                    wv[z] = a.w[iz];
+                }
+            }
+#pragma unroll
+            for (int z = 0; z < Z; ++z)
+                if (z == 0 || i + z * POLISH_STRIDE < n) s += wv[z] * x[z];
         }
         const double h0 = tm.sum(s);
         if (MODE == POLISH_EVAL_FAST) {
