@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="skip the summary of the other workloads")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--profile-case", choices=["small", "search", "extras"], default=None,
+    ap.add_argument("--profile-case", choices=["small", "search", "extras", "scoring"], default=None,
                     help="run a fixed case for ncu captures (no timing): 'small' = zeros below 1e5 x "
                          "2,048 candidates, all kernels of one plan run; 'search' = the bench workload, "
                          "each kernel launched alone once (plain; light tier at 2, 3, 4 candidates per "
@@ -778,6 +778,21 @@ def run_profile_extras():
     print(json.dumps({"profile_case": "extras", "screen_hits": int(len(r.hits))}), flush=True)
 
 
+def run_profile_scoring():
+    """The drivers' scoring at a capture-sized scale: 64 candidates over 600,000 zeros under the JP
+    weight, mb_polish_peaks_weights twice (an exact_ab_kernel and one A/B-matrix polish each;
+    ~0.7 GB on the device)."""
+    from mertens_bound_b200 import k2, path1, score, synth
+    d = synth.make_table(600_000, seed=1)
+    c = synth.make_candidates(64, seed=6)
+    c.delta[:] = np.random.default_rng(6).uniform(-1e-4, 1e-4, 64)
+    with k2.ZeroTable.from_data(d) as t:
+        s = t.add_weights(score.reference_weights(d.gamma)["jp"])
+        for _ in range(2):
+            r = path1.polish_peaks_weights(t, c, [s])
+    print(json.dumps({"profile_case": "scoring", "h_pol0": float(r[1][0][0])}), flush=True)
+
+
 def run_profile_case(args):
     """Fixed cases for ncu captures (no timing, no bench line).
       small   zeros below 1e5, 2,048 candidates: the chosen form (light tier at 4 candidates per
@@ -787,6 +802,8 @@ def run_profile_case(args):
               light tier alone at 2, 3 and 4 candidates per thread, the heavy tier alone (~80 MB)."""
     if args.profile_case == "extras":
         return run_profile_extras()
+    if args.profile_case == "scoring":
+        return run_profile_scoring()
     import torch
     from mertens_bound_b200 import k2, synth, _lib
     from mertens_bound_b200._lib import check
