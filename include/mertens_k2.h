@@ -289,8 +289,8 @@ int mb_polish_peaks_exact(mb_table *t, int64_t P, const uint64_t *v_int, const u
  * row w for weight_slots[w]; each row equals the single-weight call).  The search drivers' step
  * (search/eval_tech1_600k.py:216-273: compute_peak_AB once, then polish_peaks_with_weights per
  * weight vector): the exact (A, B) of up to 65,535 peaks at a time is written once to a device
- * buffer of at most 4 GiB, allocated for the call and freed before it returns, and read by every
- * weight's polish. */
+ * buffer of at most 4 GiB and at most half of the device's free memory, allocated for the call and
+ * freed before it returns, and read by every weight's polish. */
 int mb_polish_peaks_weights(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
                             const double *delta, int64_t n_zeros, int n_weights, const int *weight_slots,
                             double grid_half_width, int grid_steps, double *out_h_unpol, double *out_h_pol,

@@ -345,8 +345,12 @@ extern "C" int mb_polish_peaks_weights(mb_table *h, int64_t P, const uint64_t *v
     MB_TRY(device_guard(t.device));
     ExactStage s;
     MB_TRY(stage_exact(t, P, v_int, v_frac, delta, nullptr, 0, 0, s));
+    // the matrices take at most AB_BUDGET bytes and at most half of the device's free memory
+    size_t free_b = 0, total_b = 0;
+    MB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = std::min(AB_BUDGET, free_b / 2);
     const int64_t chunk =
-        std::max<int64_t>(1, std::min<int64_t>({P, (int64_t)65535, (int64_t)(AB_BUDGET / (16 * (size_t)n_zeros))}));
+        std::max<int64_t>(1, std::min<int64_t>({P, (int64_t)65535, (int64_t)(budget / (16 * (size_t)n_zeros))}));
     const size_t out_b = (size_t)n_weights * P * 8;
     DevBuf buf;
     MB_TRY(buf.ensure(2 * ((size_t)chunk * n_zeros * 8 + 256) + 3 * (out_b + 256)));
