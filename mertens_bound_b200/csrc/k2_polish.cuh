@@ -41,6 +41,46 @@ struct Team {
     double *red;           // CTA scratch of block_sum
     double *slot;          // this CTA's two exchange slots (double-buffered)
     int parity;
+    double *redv = nullptr;    // sumv scratch: [POLISH_THREADS / 32][N]
+    double *slotv = nullptr;   // sumv exchange slots: [2][N], double-buffered by vparity
+    int vparity = 0;
+
+    // Cluster-wide sums of N values with one block reduction and one cluster barrier; each value
+    // is added in exactly the order of sum() (warp shuffle tree, warps in order, ranks in order),
+    // so the results are the bits of N separate sum() calls.
+    template <int N>
+    __device__ void sumv(double (&x)[N]) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            for (int o = 16; o > 0; o >>= 1) x[i] += __shfl_xor_sync(0xffffffffu, x[i], o);
+        __syncthreads();
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < N; ++i) redv[warp * N + i] = x[i];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < POLISH_THREADS / 32; ++w) t += redv[w * N + i];
+            x[i] = t;
+        }
+        namespace cg = cooperative_groups;
+        cg::cluster_group cl = cg::this_cluster();
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int i = 0; i < N; ++i) slotv[vparity * N + i] = x[i];
+        cl.sync();
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            double t = 0.0;
+#pragma unroll
+            for (int r = 0; r < POLISH_CLUSTER; ++r) t += *cl.map_shared_rank(&slotv[vparity * N + i], r);
+            x[i] = t;
+        }
+        vparity ^= 1;
+    }
 
     // Sum of x over all threads of the cluster; every thread of every CTA gets the same value.
     // One cluster barrier per call: a CTA rewrites a slot only after the barrier of the next
@@ -362,9 +402,10 @@ __global__ void __cluster_dims__(POLISH_CLUSTER, 1, 1) __launch_bounds__(POLISH_
     __shared__ double mom[17];
     __shared__ double best_v[POLISH_THREADS], best_h[POLISH_THREADS];
     __shared__ int best_i[POLISH_THREADS];
+    __shared__ double redv[(POLISH_THREADS / 32) * 17], slotv[2 * 17];
     namespace cg = cooperative_groups;
     const int rank = (int)cg::this_cluster().block_rank();
-    Team tm{(int64_t)rank * POLISH_THREADS + threadIdx.x, red, slot, 0};
+    Team tm{(int64_t)rank * POLISH_THREADS + threadIdx.x, red, slot, 0, redv, slotv, 0};
     const int64_t p = blockIdx.x / POLISH_CLUSTER;
     const typename Src::Peak pk = src.peak(p);
     // (-1)^m/(2m)! and (-1)^m/(2m+1)!
@@ -390,16 +431,15 @@ __global__ void __cluster_dims__(POLISH_CLUSTER, 1, 1) __launch_bounds__(POLISH_
             pw *= u2;
         }
     }
+    double cs17[17];
 #pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        const double v = tm.sum(c[m]);
-        if (threadIdx.x == 0) mom[m] = v;
-    }
+    for (int m = 0; m < 9; ++m) cs17[m] = c[m];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        const double v = tm.sum(s[m]);
-        if (threadIdx.x == 0) mom[9 + m] = v;
-    }
+    for (int m = 0; m < 8; ++m) cs17[9 + m] = s[m];
+    tm.sumv(cs17);                  // the 17 moments in one reduction
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int m = 0; m < 17; ++m) mom[m] = cs17[m];
     cg::this_cluster().sync();      // peers are done reading this CTA's slots; mom[] visible
     if (rank != 0) return;          // the grid search and the writes are rank 0's
     double bv = -1.0, hv = 0.0;
