@@ -647,6 +647,20 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
         out["enumerator_screen"] = {"leaves": len(pts), "seconds": sc_s, "leaves_per_s": len(pts) / sc_s,
                                     "hits": int(len(r.hits)), "stages": "64/128/256 zeros, 0.78/0.855/0.892",
                                     "note": "host-pointer call: includes the H2D of 16 MB of leaves; median of 3 calls"}
+        # the same screen on leaves already in HBM (mb_screen_dev), device-timed
+        dvi = torch.from_numpy(pts[:, 0].view(np.int64).copy()).to(dev)
+        dvf = torch.from_numpy(pts[:, 1].view(np.int64).copy()).to(dev)
+        cap = 1 << 16
+        dh = torch.empty(cap, dtype=torch.int64, device=dev)
+        dhs = torch.empty(cap, 3, dtype=torch.float32, device=dev)
+        dn = torch.empty(1, dtype=torch.int64, device=dev)
+
+        def screen_dev():
+            hit_polish.screen_leaves_dev(t6, dvi.data_ptr(), dvf.data_ptr(), len(pts), dh.data_ptr(),
+                                         dhs.data_ptr(), dn.data_ptr(), cap, stream=sptr)
+        ds = statistics.median(timed(screen_dev, 5, 2)) * 1e-3
+        out["enumerator_screen"].update({"device_seconds": ds, "device_leaves_per_s": len(pts) / ds,
+                                         "device_note": "mb_screen_dev on leaves in HBM, CUDA events, median of 5"})
         reft = None
         if cpu_baseline:
             try:

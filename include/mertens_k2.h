@@ -241,6 +241,17 @@ int mb_hit_scan(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v
 int mb_screen(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac, double k, uint64_t step_int,
               uint64_t step_frac, int n_stages, const int64_t *stage_end, const float *threshold, int64_t max_hits,
               int64_t *out_hits, float *out_hit_scores, int64_t *n_hits, float *out_scores);
+/* mb_screen on device leaves, asynchronous on `stream` (the GPU enumerator's loop,
+ * search/gpu_mertens_stream.cu:192-250, scores leaves it generated on the device): d_v_int and
+ * d_v_frac hold P leaves; stage_end and threshold are host arrays as above.  Hits go to d_hits /
+ * d_hit_scores (device, at most max_hits, in arbitrary order) and their total to *d_n_hits (device;
+ * above max_hits the kept subset is arbitrary); d_scores (device, nullable, P x n_stages) as
+ * out_scores.  The zero records are staged in the table's scratch buffer: calls on one table that
+ * overlap on the GPU race. */
+int mb_screen_dev(mb_table *t, int64_t P, const uint64_t *d_v_int, const uint64_t *d_v_frac, double k,
+                  uint64_t step_int, uint64_t step_frac, int n_stages, const int64_t *stage_end,
+                  const float *threshold, int64_t max_hits, int64_t *d_hits, float *d_hit_scores,
+                  unsigned long long *d_n_hits, float *d_scores, void *stream);
 
 /* ---- per-peak polish contracts of search/path1_kernel_opt.py ------------------------------
  * A_j, B_j = 2 Re, 2 Im of c_j e^{i gamma_j y} and h(ddy) = sum_j w_j (A_j cos(gamma_j ddy) -

@@ -65,6 +65,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_polish_peaks_weights": (i32, [vp, i64, vp, vp, vp, i64, i32, vp, f64, i32, vp, vp, vp]),
     "mb_fast_polish_exact": (i32, [vp, i64, vp, vp, vp, i64, i32, vp, i64, i32, vp, vp, vp]),
     "mb_screen": (i32, [vp, i64, vp, vp, f64, C.c_uint64, C.c_uint64, i32, vp, vp, i64, vp, vp, vp, vp]),
+    "mb_screen_dev": (i32, [vp, i64, vp, vp, f64, C.c_uint64, C.c_uint64, i32, vp, vp, i64, vp, vp, vp, vp, vp]),
     "compute_peak_AB": (None, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "polish_peaks_with_weights": (None, [i32, i32, vp, vp, vp, vp, f64, i32, vp, vp, vp]),
     "mb_compute_peak_AB": (i32, [i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),

@@ -130,6 +130,45 @@ __global__ void __launch_bounds__(SCREEN_THREADS) screen_kernel(const ZScreen *z
     }
 }
 
+int screen_args(const Table &t, int n_stages, const int64_t *stage_end, const float *threshold, double k,
+                int64_t P, int64_t max_hits, const char *who, ScreenArgs &sa) {
+    MB_CHECK_ARG(stage_end && threshold, "%s: null stage argument", who);
+    MB_CHECK_ARG(P >= 0 && P <= ((int64_t)1 << 31), "%s: P=%lld", who, (long long)P);
+    MB_CHECK_ARG(n_stages >= 1 && n_stages <= SCREEN_MAX_STAGES, "%s: n_stages=%d", who, n_stages);
+    MB_CHECK_ARG(std::isfinite(k) && k >= 0, "%s: k=%g", who, k);
+    MB_CHECK_ARG(max_hits >= 0, "%s: max_hits=%lld", who, (long long)max_hits);
+    sa = ScreenArgs{};
+    sa.n_stages = n_stages;
+    for (int s = 0; s < n_stages; ++s) {
+        MB_CHECK_ARG(stage_end[s] >= 1 && stage_end[s] <= SCREEN_MAX_ZEROS && stage_end[s] <= t.n &&
+                         (s == 0 || stage_end[s] > stage_end[s - 1]),
+                     "%s: stage_end[%d]=%lld must increase within [1, min(%d, n)]", who, s, (long long)stage_end[s],
+                     SCREEN_MAX_ZEROS);
+        MB_CHECK_ARG(std::isfinite(threshold[s]), "%s: threshold[%d] is not finite", who, s);
+        sa.stage_end[s] = (int)stage_end[s];
+        sa.thr[s] = threshold[s];
+    }
+    return MB_OK;
+}
+
+// Zero records into d_z, the count reset, and the screen over P device leaves, all on st.
+int launch_screen(Table &t, int64_t P, const uint64_t *d_vi, const uint64_t *d_vf, double k, uint64_t step_int,
+                  uint64_t step_frac, const ScreenArgs &sa, ZScreen *d_z, int64_t max_hits,
+                  unsigned long long *d_count, int64_t *d_hits, float *d_hsc, float *d_sc, cudaStream_t st) {
+    const int nz = sa.stage_end[sa.n_stages - 1];
+    MB_CUDA(cudaMemsetAsync(d_count, 0, 8, st));
+    screen_prep_kernel<<<(nz + 127) / 128, 128, 0, st>>>(view(t), nz, k, step_int, step_frac, d_z);
+    MB_CUDA(cudaGetLastError());
+    const size_t smem = (size_t)nz * sizeof(ZScreen);
+    MB_CUDA(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(SCREEN_MAX_ZEROS * sizeof(ZScreen))));
+    const unsigned blocks = (unsigned)((P + SCREEN_THREADS - 1) / SCREEN_THREADS);
+    screen_kernel<<<blocks, SCREEN_THREADS, smem, st>>>(d_z, nz, CandView{d_vi, d_vf, nullptr, P}, sa, max_hits,
+                                                       d_count, d_hits, d_hsc, d_sc);
+    MB_CUDA(cudaGetLastError());
+    return MB_OK;
+}
+
 }  // namespace
 }  // namespace mb
 
@@ -142,21 +181,9 @@ extern "C" int mb_screen(mb_table *h, int64_t P, const uint64_t *v_int, const ui
     const char *who = "mb_screen";
     MB_CHECK_ARG(h && v_int && v_frac && stage_end && threshold && n_hits, "%s: null argument", who);
     Table &t = table_of(h);
-    MB_CHECK_ARG(P >= 0 && P <= ((int64_t)1 << 31), "%s: P=%lld", who, (long long)P);
-    MB_CHECK_ARG(n_stages >= 1 && n_stages <= SCREEN_MAX_STAGES, "%s: n_stages=%d", who, n_stages);
-    MB_CHECK_ARG(std::isfinite(k) && k >= 0, "%s: k=%g", who, k);
     MB_CHECK_ARG(max_hits >= 0 && (max_hits == 0 || (out_hits && out_hit_scores)), "%s: hit buffers", who);
-    ScreenArgs sa{};
-    sa.n_stages = n_stages;
-    for (int s = 0; s < n_stages; ++s) {
-        MB_CHECK_ARG(stage_end[s] >= 1 && stage_end[s] <= SCREEN_MAX_ZEROS && stage_end[s] <= t.n &&
-                         (s == 0 || stage_end[s] > stage_end[s - 1]),
-                     "%s: stage_end[%d]=%lld must increase within [1, min(%d, n)]", who, s, (long long)stage_end[s],
-                     SCREEN_MAX_ZEROS);
-        MB_CHECK_ARG(std::isfinite(threshold[s]), "%s: threshold[%d] is not finite", who, s);
-        sa.stage_end[s] = (int)stage_end[s];
-        sa.thr[s] = threshold[s];
-    }
+    ScreenArgs sa;
+    MB_TRY(screen_args(t, n_stages, stage_end, threshold, k, P, max_hits, who, sa));
     *n_hits = 0;
     if (P == 0) return MB_OK;
     MB_TRY(device_guard(t.device));
@@ -176,16 +203,8 @@ extern "C" int mb_screen(mb_table *h, int64_t P, const uint64_t *v_int, const ui
     cudaStream_t st = t.stream;
     MB_CUDA(cudaMemcpyAsync(d_vi, v_int, cand, cudaMemcpyHostToDevice, st));
     MB_CUDA(cudaMemcpyAsync(d_vf, v_frac, cand, cudaMemcpyHostToDevice, st));
-    MB_CUDA(cudaMemsetAsync(d_count, 0, 8, st));
-    screen_prep_kernel<<<(nz + 127) / 128, 128, 0, st>>>(view(t), nz, k, step_int, step_frac, d_z);
-    MB_CUDA(cudaGetLastError());
-    const size_t smem = (size_t)nz * sizeof(ZScreen);
-    MB_CUDA(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(SCREEN_MAX_ZEROS * sizeof(ZScreen))));
-    const unsigned blocks = (unsigned)((P + SCREEN_THREADS - 1) / SCREEN_THREADS);
-    screen_kernel<<<blocks, SCREEN_THREADS, smem, st>>>(d_z, nz, CandView{d_vi, d_vf, nullptr, P}, sa, max_hits,
-                                                       d_count, d_hits, d_hsc, d_sc);
-    MB_CUDA(cudaGetLastError());
+    MB_TRY(launch_screen(t, P, d_vi, d_vf, k, step_int, step_frac, sa, d_z, max_hits, d_count, d_hits, d_hsc,
+                         d_sc, st));
     unsigned long long total = 0;
     MB_CUDA(cudaMemcpyAsync(&total, d_count, 8, cudaMemcpyDeviceToHost, st));
     if (out_scores) MB_CUDA(cudaMemcpyAsync(out_scores, d_sc, sc_bytes, cudaMemcpyDeviceToHost, st));
@@ -211,5 +230,28 @@ extern "C" int mb_screen(mb_table *h, int64_t P, const uint64_t *v_int, const ui
                   (long long)max_hits);
         return MB_ERR_CAPACITY;
     }
+    return MB_OK;
+}
+
+extern "C" int mb_screen_dev(mb_table *h, int64_t P, const uint64_t *d_v_int, const uint64_t *d_v_frac, double k,
+                             uint64_t step_int, uint64_t step_frac, int n_stages, const int64_t *stage_end,
+                             const float *threshold, int64_t max_hits, int64_t *d_hits, float *d_hit_scores,
+                             unsigned long long *d_n_hits, float *d_scores, void *stream) {
+    const char *who = "mb_screen_dev";
+    MB_CHECK_ARG(h && d_v_int && d_v_frac && d_n_hits, "%s: null argument", who);
+    MB_CHECK_ARG(max_hits == 0 || (d_hits && d_hit_scores), "%s: hit buffers", who);
+    Table &t = table_of(h);
+    ScreenArgs sa;
+    MB_TRY(screen_args(t, n_stages, stage_end, threshold, k, P, max_hits, who, sa));
+    MB_TRY(device_guard(t.device));
+    const cudaStream_t st = (cudaStream_t)stream;
+    if (P == 0) {
+        MB_CUDA(cudaMemsetAsync(d_n_hits, 0, 8, st));
+        return MB_OK;
+    }
+    const int nz = sa.stage_end[n_stages - 1];
+    MB_TRY(t.work.ensure(nz * sizeof(ZScreen)));
+    MB_TRY(launch_screen(t, P, d_v_int, d_v_frac, k, step_int, step_frac, sa, (ZScreen *)t.work.p, max_hits,
+                         d_n_hits, d_hits, d_hit_scores, d_scores, st));
     return MB_OK;
 }

@@ -141,3 +141,20 @@ def screen_leaves(table: k2.ZeroTable, points: np.ndarray, k: float = 3e-9, stag
                           ptr(thr), cap, ptr(hits), ptr(hsc), ptr(n), ptr(sc)))
     m = int(n[0])
     return ScreenResult(hits[:m].copy(), hsc[:m].copy(), sc)
+
+
+def screen_leaves_dev(table: k2.ZeroTable, d_v_int: int, d_v_frac: int, P: int, d_hits: int, d_hit_scores: int,
+                      d_n_hits: int, max_hits: int, k: float = 3e-9, stages=SCREEN_GPU, step: float = SCREEN_STEP,
+                      d_scores: int = 0, stream: int = 0) -> None:
+    """screen_leaves on device arrays (pointers as ints: P u64 v_int and v_frac leaves; max_hits
+    int64 hit slots, max_hits x n_stages float32 hit scores, one u64 hit count; optional P x
+    n_stages float32 scores), asynchronous on `stream`; the hits come in arbitrary order."""
+    ends, thr = stages
+    ends = np.ascontiguousarray(ends, dtype=np.int64)
+    thr = np.ascontiguousarray(thr, dtype=np.float32)
+    if ends.shape != thr.shape or ends.ndim != 1:
+        raise ValueError("stage ends and thresholds must be 1-D of equal length")
+    st = _fixed(step)
+    check(lib().mb_screen_dev(table.handle, int(P), d_v_int, d_v_frac, float(k), st >> 64, st & MASK64,
+                              ends.shape[0], ptr(ends), ptr(thr), int(max_hits), d_hits, d_hit_scores, d_n_hits,
+                              d_scores or None, stream))

@@ -89,3 +89,31 @@ def test_screen_ragged_batch(table):
     a = hit_polish.screen_leaves(table, pts, stages=((64, 128), (0.2, 0.3)), all_scores=True)
     b = hit_polish.screen_leaves(table, pts[:999], stages=((64, 128), (0.2, 0.3)), all_scores=True)
     assert np.array_equal(a.scores[:999], b.scores)
+
+
+def test_screen_device_pointers(table):
+    """mb_screen_dev on device leaves gives the host call's scores, hit set and per-hit scores
+    (hits in arbitrary order on the device), twice in a row on the same buffers."""
+    import torch
+    pts = points(3000, seed=29)
+    stages = ((64, 128, 256), (0.2, 0.3, 0.35))
+    host = hit_polish.screen_leaves(table, pts, stages=stages, all_scores=True)
+    assert 0 < len(host.hits) < len(pts)
+    dev = torch.device("cuda", 0)
+    vi = torch.from_numpy(pts[:, 0].view(np.int64).copy()).to(dev)
+    vf = torch.from_numpy(pts[:, 1].view(np.int64).copy()).to(dev)
+    cap = len(pts)
+    hits = torch.empty(cap, dtype=torch.int64, device=dev)
+    hsc = torch.empty(cap, 3, dtype=torch.float32, device=dev)
+    cnt = torch.empty(1, dtype=torch.int64, device=dev)
+    sc = torch.empty(len(pts), 3, dtype=torch.float32, device=dev)
+    for _ in range(2):
+        hit_polish.screen_leaves_dev(table, vi.data_ptr(), vf.data_ptr(), len(pts), hits.data_ptr(),
+                                     hsc.data_ptr(), cnt.data_ptr(), cap, stages=stages, d_scores=sc.data_ptr())
+        torch.cuda.synchronize(dev)
+        n = int(cnt.item())
+        assert n == len(host.hits)
+        order = np.argsort(hits[:n].cpu().numpy())
+        assert np.array_equal(hits[:n].cpu().numpy()[order], host.hits)
+        assert np.array_equal(hsc[:n].cpu().numpy()[order], host.hit_scores)
+        assert np.array_equal(sc.cpu().numpy(), host.scores)
