@@ -83,3 +83,19 @@ def test_weights_call_in_chunks(gpu):
     np.testing.assert_allclose(hu[0], gu, rtol=0, atol=1e-15)
     np.testing.assert_allclose(hp[0], gp, rtol=0, atol=1e-15)
     np.testing.assert_allclose(dp[0], gd, rtol=0, atol=1e-15)
+
+
+def test_weights_call_arguments(setup):
+    """mb_polish_peaks_weights rejects an empty or oversized weight list and unknown slots; no
+    candidates give empty rows."""
+    from mertens_bound_b200._lib import K2Error
+    t, cd, table = setup
+    s = table.add_weights(score.reference_weights(t.gamma)["jp"])
+    with pytest.raises(K2Error):
+        path1.polish_peaks_weights(table, cd, [])
+    with pytest.raises(K2Error):
+        path1.polish_peaks_weights(table, cd, [s] * 65)
+    with pytest.raises(K2Error):
+        path1.polish_peaks_weights(table, cd, [s, 999])
+    hu, hp, dp = path1.polish_peaks_weights(table, cd.subset(np.arange(0)), [s, s])
+    assert hu.shape == (2, 0) and hp.shape == (2, 0) and dp.shape == (2, 0)

@@ -117,3 +117,34 @@ def test_screen_device_pointers(table):
         assert np.array_equal(hits[:n].cpu().numpy()[order], host.hits)
         assert np.array_equal(hsc[:n].cpu().numpy()[order], host.hit_scores)
         assert np.array_equal(sc.cpu().numpy(), host.scores)
+
+
+def test_screen_device_edges(table):
+    """mb_screen_dev: no leaves gives a zero count; a hit buffer smaller than the hits keeps that
+    many (a subset of the host call's hits) and reports the full count; argument errors raise."""
+    import torch
+    dev = torch.device("cuda", 0)
+    pts = points(2000, seed=31)
+    stages = ((64, 128, 256), (0.2, 0.3, 0.35))
+    host = hit_polish.screen_leaves(table, pts, stages=stages)
+    assert len(host.hits) > 3
+    vi = torch.from_numpy(pts[:, 0].view(np.int64).copy()).to(dev)
+    vf = torch.from_numpy(pts[:, 1].view(np.int64).copy()).to(dev)
+    hits = torch.empty(2, dtype=torch.int64, device=dev)
+    hsc = torch.empty(2, 3, dtype=torch.float32, device=dev)
+    cnt = torch.full((1,), 7, dtype=torch.int64, device=dev)
+    hit_polish.screen_leaves_dev(table, vi.data_ptr(), vf.data_ptr(), 0, hits.data_ptr(), hsc.data_ptr(),
+                                 cnt.data_ptr(), 2, stages=stages)
+    torch.cuda.synchronize(dev)
+    assert int(cnt.item()) == 0
+    hit_polish.screen_leaves_dev(table, vi.data_ptr(), vf.data_ptr(), len(pts), hits.data_ptr(), hsc.data_ptr(),
+                                 cnt.data_ptr(), 2, stages=stages)
+    torch.cuda.synchronize(dev)
+    assert int(cnt.item()) == len(host.hits)
+    assert set(hits.cpu().numpy().tolist()) <= set(host.hits.tolist())
+    with pytest.raises(K2Error):
+        hit_polish.screen_leaves_dev(table, vi.data_ptr(), vf.data_ptr(), len(pts), hits.data_ptr(),
+                                     hsc.data_ptr(), cnt.data_ptr(), 2, stages=((128, 64), (0.1, 0.2)))
+    with pytest.raises(K2Error):
+        hit_polish.screen_leaves_dev(table, vi.data_ptr(), vf.data_ptr(), len(pts), 0, 0, cnt.data_ptr(), 2,
+                                     stages=stages)
