@@ -47,10 +47,10 @@ WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 can
 # gamma = 3.29e6) for each candidates-per-thread setting -- and their DRAM bytes per launch on this
 # workload, from the ncu capture of `bench.py --profile-case search` summarised in
 # profiles/k2_light_kernel_search_scoring.md.
-LIGHT_INST_PER_TERM = {2: 21.39, 3: 21.50, 4: 17.97}
+LIGHT_INST_PER_TERM = {2: 19.75, 3: 20.29, 4: 16.87}
 HEAVY_INST_PER_TERM = 41.04
-LIGHT_DRAM_BYTES = {2: 16486656, 3: 16500480, 4: 16445952}
-HEAVY_DRAM_BYTES = 2775552
+LIGHT_DRAM_BYTES = {2: 16487680, 3: 16464128, 4: 16447232}
+HEAVY_DRAM_BYTES = 2774784
 REF_SAMPLE_CANDS = 64
 
 

@@ -75,8 +75,8 @@ MB_DEV void light_tile(const void *tile_v, int nt, int zl, int ZL, const CandReg
     float acc[CPT][3];
 #pragma unroll
     for (int i = 0; i < CPT; ++i) acc[i][0] = acc[i][1] = acc[i][2] = 0.f;
-    int cnt = 0;
-    for (int jj = zl; jj < nt; jj += ZL) {
+    // one zero's terms for every candidate of the thread
+    auto term = [&](int jj) {
         const Rec z = tile[jj];
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
@@ -91,21 +91,25 @@ MB_DEV void light_tile(const void *tile_v, int nt, int zl, int ZL, const CandReg
             acc[i][1] = fmaf(z.b, s, acc[i][1]);
             acc[i][2] = fmaf(z.d, co, acc[i][2]);
         }
-        if (++cnt == LIGHT_FLUSH) {
-            cnt = 0;
+    };
+    auto flush = [&]() {
 #pragma unroll
-            for (int i = 0; i < CPT; ++i)
+        for (int i = 0; i < CPT; ++i)
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    sum[i][q] += (double)acc[i][q];
-                    acc[i][q] = 0.f;
-                }
-        }
+            for (int q = 0; q < 3; ++q) {
+                sum[i][q] += (double)acc[i][q];
+                acc[i][q] = 0.f;
+            }
+    };
+    // whole groups of LIGHT_FLUSH zeros (a fixed trip count, no per-zero counter), then the rest
+    int jj = zl;
+    for (; jj + (LIGHT_FLUSH - 1) * ZL < nt; jj += LIGHT_FLUSH * ZL) {
+#pragma unroll 1
+        for (int q = 0; q < LIGHT_FLUSH; ++q) term(jj + q * ZL);
+        flush();
     }
-#pragma unroll
-    for (int i = 0; i < CPT; ++i)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) sum[i][q] += (double)acc[i][q];
+    for (; jj < nt; jj += ZL) term(jj);
+    flush();
 }
 
 // sin/cos(2 pi y) for any y (turns): y = q/1024 + r with |r| <= 2^-11 (exact), the table
