@@ -623,6 +623,30 @@ def other_workloads(torch, dev, timed, cpu_baseline: bool = True):
             ds["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
     out["driver_scoring"] = ds
 
+    # driver_dropin: the same step with the drivers unchanged, through the library's
+    # compute_peak_AB / polish_peaks_with_weights (search/eval_tech1_600k.py:216-273 calling
+    # libmertens_k2.so in place of libpath1_eval.so): the A and B matrices of 64 candidates
+    # (2 x 307 MB) come to the host once and go back to the device for each of the five polishes
+    from mertens_bound_b200 import compat, formats
+    f6 = formats.reference_fields(d600, exact_psi=False)
+    sub = c6.subset(np.arange(64))
+    xs = [(int(a) << 30) | (int(b) >> 34) for a, b in zip(sub.v_int, sub.v_frac)]
+    x_lo = np.array([v & 0xFFFFFFFFFFFFFFFF for v in xs], np.uint64)
+    x_hi = np.array([v >> 64 for v in xs], np.uint64)
+    dy0 = np.array([int(b) & ((1 << 34) - 1) for b in sub.v_frac], dtype=np.float64) * 2.0 ** -64 + sub.delta
+
+    def dropin():
+        A, B = compat.compute_peak_AB(x_lo, x_hi, dy0, f6["alpha"], f6["gamma"], f6["ghi_lo"], f6["ghi_hi"],
+                                      f6["glo_lo"], f6["glo_hi"], f6["psi_lo"], f6["psi_hi"])
+        return [compat.polish_peaks_with_weights(A, B, d600.gamma, w, 2.5e-4, 40) for w in W.values()]
+    dropin()
+    t0 = time.perf_counter()
+    dropin()
+    di_s = time.perf_counter() - t0
+    out["driver_dropin"] = {"candidates": 64, "zeros": 600_000, "seconds": di_s, "candidates_per_s": 64 / di_s,
+                            "note": "unchanged drivers through the compute_peak_AB / polish_peaks_with_weights "
+                                    "exports: host A/B matrices cross PCIe once out and five times in"}
+
     # the enumerators' two GPU steps and the peak re-optimisation, each on the 600,000-zero table:
     #   enumerator_screen  2^20 random leaves through the GPU screen (64/128/256 zeros, 7 offsets)
     #   hit_polish         256 hits through the five ZeroData::polish stages
