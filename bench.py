@@ -311,7 +311,8 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "int32 phase + f64 (heavy tier) + f32 (light tier)",
         "data": "synthetic (seeded zero table and candidates; no real zeta zeros)",
         "config": {"workload": WORKLOAD, "zeros": n_T, "candidates_per_gpu": P, "k": K_GAUSS, "T0": T0,
-                   "tol": TOL, "heavy_zeros": gi["n_heavy"], "err_bound": gi["err_bound"],
+                   "tol": TOL, "heavy_zeros": gi["n_heavy"], "light_form": plan.info()["light_form"],
+                   "err_bound": gi["err_bound"],
                    "err_bound_dd": gi["err_bound_dd"], "err_bound_dk": gi["err_bound_dk"],
                    "l2": "256 MB buffer written between timed steps (table 28 MB < L2)",
                    "parallelism": f"candidates sharded over {world} GPU(s), no collective on the data path",

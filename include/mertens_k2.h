@@ -177,6 +177,10 @@ int mb_plan_set_zero_range(mb_plan *p, int64_t j0, int64_t j1);
 /* Median device time in ms of `reps` runs on synthetic candidates (for the autotuner). */
 int mb_plan_time(mb_plan *p, int reps, double *ms);
 int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, int *n_items);
+/* *fused = 1 when the plan's light tier takes the fraction part of v through one FMA (every zero
+ * of its table below gamma = 2 pi (2^19 - 1) = 3.29e6), 0 for the split form.  Plan introspection;
+ * no counterpart in the reference. */
+int mb_plan_light_form(const mb_plan *p, int *fused);
 int mb_plan_group_info(const mb_plan *p, int g, int64_t *n_T, int64_t *n_heavy, double *err_bound,
                        double *sum_abs);
 /* Device pointers (P = sum of counts), asynchronous on `stream`. */

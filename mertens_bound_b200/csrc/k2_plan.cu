@@ -529,6 +529,12 @@ extern "C" int mb_plan_info(const mb_plan *p, int64_t *P, double *zero_terms, in
     return MB_OK;
 }
 
+extern "C" int mb_plan_light_form(const mb_plan *p, int *fused) {
+    MB_CHECK_ARG(p && fused, "mb_plan_light_form: null argument");
+    *fused = p->dev.fused_phase ? 1 : 0;
+    return MB_OK;
+}
+
 extern "C" int mb_plan_group_info(const mb_plan *p, int g, int64_t *n_T, int64_t *n_heavy,
                                   double *err_bound, double *sum_abs) {
     MB_CHECK_ARG(p && g >= 0 && g < p->n_groups, "mb_plan_group_info: bad plan/group");

@@ -190,9 +190,13 @@ class Plan:
         return h.value, l.value
 
     def info(self):
-        P, zt, ni = C.c_int64(), C.c_double(), C.c_int()
+        """P, zero_terms, n_items and light_form: "fused" (the light tier's one-FMA fraction product,
+        every zero of the table below gamma = 3.29e6) or "split"."""
+        P, zt, ni, fu = C.c_int64(), C.c_double(), C.c_int(), C.c_int()
         check(_lib.lib().mb_plan_info(self.handle, C.byref(P), C.byref(zt), C.byref(ni)))
-        return {"P": P.value, "zero_terms": zt.value, "n_items": ni.value}
+        check(_lib.lib().mb_plan_light_form(self.handle, C.byref(fu)))
+        return {"P": P.value, "zero_terms": zt.value, "n_items": ni.value,
+                "light_form": "fused" if fu.value else "split"}
 
     def group_info(self, g: int):
         nT, nh, eb, sa = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()

@@ -50,6 +50,7 @@ def test_batched_plan_groups(table):
     P = sum(counts)
     cd = synth.make_candidates(P, seed=8)
     with k2.Plan(table, counts, ks, Ts, tol=TOL) as plan:
+        assert plan.info()["light_form"] == "fused"        # every zero of the table below 3.29e6
         val, dd, dk = plan.run(cd)
         val2, _, _ = plan.run(cd)            # graph replay gives identical results
         assert np.array_equal(val, val2)
@@ -220,6 +221,7 @@ def test_high_gamma_table(gpu, small_table, oracle, tol):
         val, dd, dk, eb = k2.k2_fast(t, cd, 0.0, tol=tol)
         with k2.Plan(t, [64], [0.0], [math.inf], tol=tol) as plan:
             gi = plan.group_info(0)
+            assert plan.info()["light_form"] == "split"
     assert gi["n_heavy"] < data.n and (gi["n_heavy"] > 0) == (tol < 1e-6)
     assert eb <= tol
     assert np.max(np.abs(val - ohi[:, 0])) <= eb
