@@ -27,9 +27,7 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -42,15 +40,22 @@ UNIT = "zero-terms/s"
 T0, K_GAUSS, P_PER_GPU, TOL = 3e5, 3e-9, 4096, 1e-10
 WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 candidates v~3.5e18 "
             "per GPU, k=3e-9, K2 + dK2/ddelta + dK2/dk per candidate, a-priori |err| <= 1e-10")
-# Warp instructions per warp of zero-terms (= thread instructions per zero-term) of the two
-# tier kernels -- the light tier (its one-FMA fraction product, as every zero here lies below
-# gamma = 3.29e6) for each candidates-per-thread setting -- and their DRAM bytes per launch on this
-# workload, from the ncu capture of `bench.py --profile-case search` summarised in
-# profiles/k2_light_kernel_search_scoring.md.
-LIGHT_INST_PER_TERM = {2: 19.75, 3: 20.29, 4: 16.87}
-HEAVY_INST_PER_TERM = 41.04
+# Per-launch DRAM bytes of the two tier kernels on this workload (light tier at each
+# candidates-per-thread setting, its one-FMA fraction product), from one ncu capture of
+# `bench.py --profile-case search` (dram__bytes_read.sum + dram__bytes_write.sum), and the
+# executed thread instructions per zero-term of each kernel from the same capture
+# (smsp__inst_executed.sum x 32 / zero-terms): the issue-slot side figure beside the pipe roofline.
 LIGHT_DRAM_BYTES = {2: 16487680, 3: 16464128, 4: 16447232}
 HEAVY_DRAM_BYTES = 2774784
+LIGHT_INST_PER_TERM = {2: 19.75, 3: 20.29, 4: 16.87}
+HEAVY_INST_PER_TERM = 41.04
+# Algorithmic operations per zero-term on each tier's binding pipe:
+#   light tier, XU (MUFU) pipe: one sine and one cosine of the reduced phase;
+#   heavy tier, FP64 pipe: 4 DFMA for the 2^-64 phase products, 1 for the phase sum, 12 for the
+#   table sine/cosine (index, remainder, r^2, two short polynomials, two rotations) and 3 FMA
+#   accumulations of K2, dK2/ddelta, dK2/dk.
+LIGHT_MUFU_PER_TERM = 2
+HEAVY_FP64_PER_TERM = 20
 REF_SAMPLE_CANDS = 64
 
 
@@ -79,54 +84,81 @@ CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.ac
 
 
 class ClockSampler:
-    def __init__(self, gpu_index: int):
-        self.path = tempfile.mktemp(prefix="mb_clocks_", suffix=".csv")
-        self.f = open(self.path, "w")
+    """SM clock and clock-event reasons of one GPU, read through NVML every `period` seconds on a
+    background thread between construction and stop() (the timed region)."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, cuda_index: int, period: float = 0.002):
+        import threading
+        self.sm, self.masks, self.max_mhz, self.error = [], [], None, None
+        self._stop = threading.Event()
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={CLOCK_QUERY}",
-                                       "--format=csv,noheader,nounits", "-lms", "50"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
-        except FileNotFoundError:
-            self.p = None
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = self._handle(pynvml, cuda_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.bits = {name: getattr(pynvml, const) for name, const in self.REASONS}
+        except Exception as e:                                   # no NVML: the line says so
+            self.error = f"{type(e).__name__}: {e}"
+            self.h = None
+        self.t = threading.Thread(target=self._run, args=(period,), daemon=True)
+        if self.h is not None:
+            self._sample()                                       # at least one sample in the region
+            self.t.start()
+
+    @staticmethod
+    def _handle(pynvml, cuda_index: int):
+        """The NVML handle of CUDA device cuda_index (matched by PCI bus id, so a
+        CUDA_VISIBLE_DEVICES mapping does not matter)."""
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(cuda_index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(cuda_index)
+
+    def _sample(self):
+        nv = self.nv
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        self.masks.append(int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+
+    def _run(self, period):
+        while not self._stop.wait(period):
+            try:
+                self._sample()
+            except Exception as e:
+                self.error = f"{type(e).__name__}: {e}"
+                return
 
     def stop(self) -> dict:
-        if self.p is not None:
-            self.p.terminate()
-            try:
-                self.p.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.p.kill()
-        self.f.close()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        try:
-            for line in open(self.path):
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    mx = float(parts[2])
-                except ValueError:
-                    continue
-                for n, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(n)
-        finally:
-            try:
-                os.unlink(self.path)
-            except OSError:
-                pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        if self.h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": [], "error": self.error}
+        self._sample()
+        self._stop.set()
+        self.t.join(timeout=5)
+        reasons = sorted(n for n, b in self.bits.items() if any(m & b for m in self.masks))
+        out = {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.max_mhz, "samples": len(self.sm),
+               "sm_mhz_min": min(self.sm), "reasons": reasons, "source": "NVML, sampled on a thread"}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 # ---------------------------------------------------------------- reference CPU evaluator
 
-def reference_rate(table, cands, k: float, n_use: int, seconds: float, steps: int | None = None):
+def reference_rate(table, cands, k: float, n_use: int, seconds: float, steps: int | None = None,
+                   per_step: int = REF_SAMPLE_CANDS):
     """Zero-terms/s of the reference's compute_peak_AB plus the value and gradient sums
     (h0 = sum w A as in path1_eval_fast.cpp:76-81, dK2/dv = -sum w gamma B,
-    dK2/dk = -sum w gamma^2 A) on REF_SAMPLE_CANDS candidates per call."""
+    dK2/dk = -sum w gamma^2 A) as NumPy dots.  A step is per_step candidates in calls of
+    REF_SAMPLE_CANDS candidates (the P x N A/B matrices of a whole step would not fit in memory);
+    it runs `steps` steps, or steps until `seconds` have been spent."""
     from oracle.oracle import Oracle, RefLib, reference_candidates, reference_format
 
     reft = reference_format(table, n_use, exact_psi=False)
@@ -139,36 +171,55 @@ def reference_rate(table, cands, k: float, n_use: int, seconds: float, steps: in
         O, kind, cores = Oracle(), "port", 1
         peak_ab = lambda refc: O.ref_peak_AB(refc, reft)
     P = cands.n
-    done, t_total, calls = 0, 0.0, 0
+    done, t_total, n_steps = 0, 0.0, 0
     idx = 0
     while True:
-        sel = np.arange(idx, idx + REF_SAMPLE_CANDS) % P
-        idx += REF_SAMPLE_CANDS
-        refc = reference_candidates(cands.subset(sel))
-        t = time.perf_counter()
-        A, B = peak_ab(refc)
-        h0, dd, dk = A @ w, -(B @ wg), -(A @ wg2)
-        t_total += time.perf_counter() - t
-        done += REF_SAMPLE_CANDS * n_use
-        calls += 1
-        if (steps is not None and calls >= steps) or (steps is None and t_total >= seconds):
+        for c0 in range(0, per_step, REF_SAMPLE_CANDS):
+            m = min(REF_SAMPLE_CANDS, per_step - c0)
+            sel = np.arange(idx, idx + m) % P
+            idx += m
+            refc = reference_candidates(cands.subset(sel))
+            t = time.perf_counter()
+            A, B = peak_ab(refc)
+            h0, dd, dk = A @ w, -(B @ wg), -(A @ wg2)
+            t_total += time.perf_counter() - t
+            done += m * n_use
+        n_steps += 1
+        if (steps is not None and n_steps >= steps) or (steps is None and t_total >= seconds):
             break
-    return done / t_total, kind, cores, calls, t_total
+    return done / t_total, kind, cores, n_steps, t_total
+
+
+def reference_polish_form(table, cands, k: float, n_use: int) -> dict:
+    """The other form of the reference's h0: compute_peak_AB, then polish_peaks_with_weights with
+    grid_steps = 0 (path1_eval_fast.cpp:58-143; it returns h0 in out_h_unpol and also runs its
+    Newton passes), on one call of REF_SAMPLE_CANDS candidates; zero-terms counted as for the
+    NumPy form (candidates x zeros)."""
+    from oracle.oracle import RefLib, reference_candidates, reference_format
+    if not RefLib.available():
+        return {"unavailable": "oracle/_ref/libpath1_eval.so not built"}
+    R = RefLib()
+    reft = reference_format(table, n_use, exact_psi=False)
+    w = np.exp(-k * table.gamma[:n_use] ** 2)
+    refc = reference_candidates(cands.subset(np.arange(REF_SAMPLE_CANDS)))
+    t = time.perf_counter()
+    A, B = R.peak_AB(refc, reft)
+    R.polish(A, B, table.gamma[:n_use], w, 0.0, 0)
+    secs = time.perf_counter() - t
+    return {"value": REF_SAMPLE_CANDS * n_use / secs, "seconds": secs,
+            "sample": f"{REF_SAMPLE_CANDS} candidates x {n_use} zeros: compute_peak_AB + "
+                      "polish_peaks_with_weights(grid_steps=0), value only"}
+
+
+def workload_config(world: int, n_T: int) -> dict:
+    """The workload both arms run (the same dict in both lines)."""
+    return {"workload": WORKLOAD, "zeros": n_T, "candidates_per_gpu": P_PER_GPU, "k": K_GAUSS, "T0": T0,
+            "tol": TOL, "l2": "GPU arm: a 256 MB buffer written between timed steps (the 28 MB table "
+                              "would otherwise stay in the 126 MB L2)",
+            "parallelism": f"candidates sharded over {world} GPU(s), no collective on the data path"}
 
 
 # ---------------------------------------------------------------- our arm
-
-def hbm_line(bytes_per_launch: float, ms: float) -> dict:
-    """The light kernel's DRAM traffic as a fraction of the measured HBM copy peak (it is not the
-    binding roof: the kernel is issue bound)."""
-    gbs = bytes_per_launch / (ms * 1e-3) / 1e9
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peak, src = float(json.load(f)["hbm_gbs"]), "measured"
-    except (OSError, KeyError, ValueError):
-        peak, src = 6650.0, "fallback"
-    return {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak, "peak_source": src}
-
 
 def run_ours(args):
     import torch
@@ -244,9 +295,12 @@ def run_ours(args):
         check(L.mb_plan_run_tiers_dev(plan.handle, tiers, vi.data_ptr(), vf.data_ptr(), dl.data_ptr(),
                                       out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), sptr))
 
-    # headline: chosen form, exactly K timed steps bracketed by barrier + synchronize
+    # headline: chosen form, exactly K timed steps bracketed by barrier + synchronize; the plan
+    # records CUDA events around each step's light and heavy launches (the kernels' own durations
+    # inside the concurrent step, on the streams they run on)
     for _ in range(max(3, args.warmup)):
         fast()
+    check(L.mb_plan_kernel_timing(plan.handle, args.steps))
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
@@ -260,6 +314,8 @@ def run_ours(args):
     total_ms = max_over_ranks(sum(step_ms))
     value = world * terms * args.steps / (total_ms * 1e-3)
     ms_per_step = total_ms / args.steps
+    light_in_step, heavy_in_step = kernel_times(L, plan, args.steps)
+    check(L.mb_plan_kernel_timing(plan.handle, 0))
     diff = (out - ref).abs().max(dim=1).values.cpu().numpy()
     # error against rigorous enclosures: the certified interval kernel on a 64-candidate subsample
     # (the error of a value inside nothing wider than the interval is below |val - mid| + width/2)
@@ -267,21 +323,13 @@ def run_ours(args):
     clo, chi, _ = k2.k2_certified(table, sub, K_GAUSS, T0)
     got = out[0, :64].cpu().numpy()
     mid, half = 0.5 * (clo + chi), 0.5 * (chi - clo)
-    err_vs_cert = {"candidates": 64, "max_abs_err": float(np.max(np.abs(got - mid) + half)),
-                   "max_interval_width": float(np.max(chi - clo)), "a_priori_bound": gi["err_bound"]}
+    err_vs_cert = float(np.max(np.abs(got - mid) + half))
 
-    # per-tier kernels on their own (roofline of the dominant kernel)
+    # per-tier kernels on their own
     light_ms = statistics.median(timed(lambda: fast(2), 5, 1))
     heavy_ms = statistics.median(timed(lambda: fast(1), 5, 1))
     ht, lt = C_double_pair(L.mb_plan_tier_terms, plan.handle)
-    peak = C_double(L.mb_calibrate_issue, local)
-    # the timed step runs the two tier kernels concurrently (plus a small reduction): the roof is
-    # the instruction issue of the whole step; the light kernel alone is reported beside it
-    cpt = tuned["config"][0]
-    inst_per_term = LIGHT_INST_PER_TERM[cpt]
-    step_inst = inst_per_term * lt + HEAVY_INST_PER_TERM * ht
-    step_achieved = step_inst / (ms_per_step * 1e-3)
-    light_achieved = inst_per_term * lt / (light_ms * 1e-3)
+    ffma_peak, mufu_peak, dfma_peak = calibrate_pipes(L, local)
 
     # end to end through the host-pointer API (pinned H2D, graph, D2H), every step
     for _ in range(3):
@@ -304,48 +352,67 @@ def run_ours(args):
                  "speedup_vs_full_step": ms_per_step / skip_ms}
     plan.set_skip(0.0)
 
-    plain_rate = terms / (statistics.median(plain_ms) * 1e-3)
+    plain_step_ms = statistics.median(plain_ms)
+    plain_rate = terms / (plain_step_ms * 1e-3)
+    cpt = tuned["config"][0]
+    light_mean = statistics.fmean(light_in_step)
+    heavy_mean = statistics.fmean(heavy_in_step)
+    mufu_achieved = LIGHT_MUFU_PER_TERM * lt / (light_mean * 1e-3)
+    fp64_achieved = HEAVY_FP64_PER_TERM * ht / (heavy_mean * 1e-3)
+    # the dominant kernel: the light tier (its launch spans most of the step); its binding pipe is
+    # XU (two MUFU operations per zero-term), against the XU rate measured live on this GPU
+    roofline = {
+        "bound": "xu", "kernel": "k2_light_kernel (light tier), inside the concurrent step",
+        "achieved": mufu_achieved / 1e12, "peak": mufu_peak / 1e12, "unit": "T MUFU-op/s",
+        "frac": mufu_achieved / mufu_peak,
+        "traffic": LIGHT_DRAM_BYTES[cpt], "traffic_unit": "bytes/launch (ncu dram read+write)",
+        "algorithmic": f"{LIGHT_MUFU_PER_TERM} MUFU (sin, cos) per light zero-term",
+        "peak_source": "measured live: sin.approx/cos.approx chains (mb_calibrate_pipes)",
+        "light_terms": lt, "light_ms_in_step": light_mean,
+        "light_alone_ms": light_ms, "light_alone_frac": LIGHT_MUFU_PER_TERM * lt / (light_ms * 1e-3) / mufu_peak,
+        "heavy_terms": ht, "heavy_ms_in_step": heavy_mean, "heavy_alone_ms": heavy_ms,
+        "heavy_fp64_achieved": fp64_achieved / 1e12, "heavy_fp64_peak": dfma_peak / 1e12,
+        "heavy_fp64_frac": fp64_achieved / dfma_peak,
+        "heavy_alone_fp64_frac": HEAVY_FP64_PER_TERM * ht / (heavy_ms * 1e-3) / dfma_peak,
+        "heavy_traffic": HEAVY_DRAM_BYTES,
+        "step_xu_frac": LIGHT_MUFU_PER_TERM * lt / (ms_per_step * 1e-3) / mufu_peak,
+        "step_fp64_frac": HEAVY_FP64_PER_TERM * ht / (ms_per_step * 1e-3) / dfma_peak,
+        "issue_frac_side": (LIGHT_INST_PER_TERM[cpt] * lt + HEAVY_INST_PER_TERM * ht) / (ms_per_step * 1e-3)
+                           / ffma_peak,
+        "hbm_frac_side": (LIGHT_DRAM_BYTES[cpt] + HEAVY_DRAM_BYTES) / (ms_per_step * 1e-3) / 1e9 / hbm_peak()[0],
+        "plain_fp64_ms_per_step": plain_step_ms, "plain_fp64_value": world * plain_rate,
+        "speedup_vs_plain": value / (world * plain_rate),
+        "err_bound": gi["err_bound"], "err_bound_dd": gi["err_bound_dd"], "err_bound_dk": gi["err_bound_dk"],
+        "err_vs_certified_max": err_vs_cert, "max_abs_diff_vs_plain": float(diff[0]),
+        "heavy_zeros": gi["n_heavy"], "light_form": plan.info()["light_form"],
+        "tile_light_cpt": cpt, "tile_nzw_shift": tuned["config"][1], "tile_chunk_scale": tuned["config"][2],
+    }
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32 phase + f64 (heavy tier) + f32 (light tier)",
         "data": "synthetic (seeded zero table and candidates; no real zeta zeros)",
-        "config": {"workload": WORKLOAD, "zeros": n_T, "candidates_per_gpu": P, "k": K_GAUSS, "T0": T0,
-                   "tol": TOL, "heavy_zeros": gi["n_heavy"], "light_form": plan.info()["light_form"],
-                   "err_bound": gi["err_bound"],
-                   "err_bound_dd": gi["err_bound_dd"], "err_bound_dk": gi["err_bound_dk"],
-                   "l2": "256 MB buffer written between timed steps (table 28 MB < L2)",
-                   "parallelism": f"candidates sharded over {world} GPU(s), no collective on the data path",
-                   "wall_s_timed_region": wall_s,
-                   "autotuned": {"light_cpt": tuned["config"][0], "nzw_shift": tuned["config"][1],
-                                 "chunk_scale": tuned["config"][2], "tuning_s": tune_s}},
-        "plain_fp64": {"value": world * plain_rate, "ms_per_step": statistics.median(plain_ms)},
-        "speedup_vs_plain": world * plain_rate and value / (world * plain_rate),
-        "max_abs_diff_vs_plain": {"val": float(diff[0]), "dd": float(diff[1]), "dk": float(diff[2])},
-        "err_vs_certified": err_vs_cert,
+        "config": workload_config(world, n_T),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * P, "d2h_bytes_per_step": 3 * 8 * P},
-        "roofline": {"bound": "issue", "kernel": "k2_light_kernel + k2_heavy_kernel (concurrent, one step)",
-                     "achieved": step_achieved / 1e12, "peak": peak / 1e12, "unit": "T thread-inst/s",
-                     "frac": step_achieved / peak,
-                     "traffic": LIGHT_DRAM_BYTES[cpt] + HEAVY_DRAM_BYTES, "traffic_unit": "bytes/step",
-                     "inst_per_term": {"light": inst_per_term, "heavy": HEAVY_INST_PER_TERM},
-                     "light_terms": lt, "heavy_terms": ht,
-                     "light_alone": {"ms": light_ms, "achieved": light_achieved / 1e12,
-                                     "frac": light_achieved / peak},
-                     "heavy_alone_ms": heavy_ms,
-                     "peak_source": "measured live: FFMA issue rate (mb_calibrate_issue); MEASURED_PEAKS.json "
-                                    "has only HBM and bf16-tensor peaks, neither binds these kernels",
-                     "hbm": hbm_line(LIGHT_DRAM_BYTES[cpt] + HEAVY_DRAM_BYTES, ms_per_step)},
+        "roofline": roofline,
         "clocks": clocks,
         "gpu_launches": 3 * args.steps,
+        "wall_s_timed_region": wall_s,
+        "accuracy": {"err_vs_certified": {"candidates": 64, "max_abs_err": err_vs_cert,
+                                          "max_interval_width": float(np.max(chi - clo)),
+                                          "a_priori_bound": gi["err_bound"]},
+                     "max_abs_diff_vs_plain": {"val": float(diff[0]), "dd": float(diff[1]), "dk": float(diff[2])}},
+        "autotune_s": tune_s,
         "tail_skip": tail_skip,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, kind, cores, calls, secs = reference_rate(data, cands, K_GAUSS, n_T, args.cpu_seconds)
+        pf = reference_polish_form(data, cands, K_GAUSS, n_T)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                                 "sample": f"{calls} calls x {REF_SAMPLE_CANDS} candidates x {n_T} zeros "
-                                          f"({secs:.1f} s): compute_peak_AB + value/grad sums",
-                                "nproc": os.cpu_count()}
+                                          f"({secs:.1f} s): compute_peak_AB + value/grad sums as NumPy dots",
+                                "nproc": os.cpu_count(), "polish_form_value": pf.get("value"),
+                                "polish_form_sample": pf.get("sample", pf.get("unavailable"))}
     plan.close()
     table.close()
     if world == 1 and not args.no_workloads:
@@ -764,9 +831,41 @@ def C_double_pair(fn, *args):
     return a.value, b.value
 
 
+def kernel_times(L, plan, n: int):
+    """The light and heavy kernel durations (ms) of the plan's last n timed runs."""
+    import ctypes as C
+    from mertens_bound_b200._lib import check
+    lt, ht, got = (C.c_double * n)(), (C.c_double * n)(), C.c_int()
+    check(L.mb_plan_kernel_times(plan.handle, n, lt, ht, C.byref(got)))
+    if got.value != n:
+        raise RuntimeError(f"kernel timing recorded {got.value} of {n} runs")
+    return list(lt), list(ht)
+
+
+def calibrate_pipes(L, device: int):
+    """Measured FFMA, MUFU and DFMA thread-op rates of this GPU (ops/s)."""
+    import ctypes as C
+    from mertens_bound_b200._lib import check
+    f, m, d = C.c_double(), C.c_double(), C.c_double()
+    check(L.mb_calibrate_pipes(device, C.byref(f), C.byref(m), C.byref(d)))
+    return f.value, m.value, d.value
+
+
+def hbm_peak():
+    """The measured HBM copy peak (GB/s) if MEASURED_PEAKS.json holds one, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError, TypeError):
+        return 6650.0, "fallback"
+
+
 # ---------------------------------------------------------------- reference arm
 
 def run_reference(args):
+    """The reference's own evaluator on the same workload: every timed step scores all 4,096
+    candidates over the 466,659 zeros (compute_peak_AB in calls of 64 candidates plus the value and
+    gradient sums); each untimed warm-up step is one such call."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
@@ -775,17 +874,21 @@ def run_reference(args):
     data = synth.make_table_below(T0, seed=1)
     cands = synth.make_candidates(P_PER_GPU, seed=3)
     n_T = data.count_below(T0)
-    reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=max(1, args.warmup))     # warm-up
-    rate, kind, cores, calls, secs = reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=args.steps)
+    reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=max(1, args.warmup))          # warm-up
+    rate, kind, cores, n_steps, secs = reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=args.steps,
+                                                      per_step=P_PER_GPU)
+    pf = reference_polish_form(data, cands, K_GAUSS, n_T)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / calls * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / n_steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (same table and candidates as the ours arm)",
-        "config": {"workload": WORKLOAD, "zeros": n_T, "candidates_per_step": REF_SAMPLE_CANDS},
+        "data": "synthetic (seeded zero table and candidates; no real zeta zeros)",
+        "config": workload_config(world, n_T),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{REF_SAMPLE_CANDS} candidates x {n_T} zeros per step",
-                         "nproc": os.cpu_count()},
+                         "sample": f"every step: {P_PER_GPU} candidates x {n_T} zeros in calls of "
+                                   f"{REF_SAMPLE_CANDS} (compute_peak_AB + value/grad sums as NumPy dots)",
+                         "nproc": os.cpu_count(), "polish_form_value": pf.get("value"),
+                         "polish_form_sample": pf.get("sample", pf.get("unavailable"))},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

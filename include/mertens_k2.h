@@ -109,9 +109,10 @@ int mb_k2_certified_range(mb_table *t, int64_t P, const uint64_t *v_int, const u
  * n_zeros), d_gamma, d_cre, d_cim -- sums the first n_use zeros, and passes candidates and
  * outputs as device arrays.  Scratch for the partial sums is a fixed 8 MiB device array that
  * every GPU loading the library keeps until exit, so P <= 349,525 (larger P returns
- * MB_ERR_CAPACITY).  Calls that overlap on the GPU race on that array.  The first call on a
- * device looks up the array's address; make it before any stream capture.
- * Runs on the current device, asynchronously on `stream`. */
+ * MB_ERR_CAPACITY).  All calls share that array: calls that overlap on the GPU (other streams,
+ * other host threads) race on it.  The first call on a device (and the first after that
+ * device's context was replaced, e.g. by cudaDeviceReset) looks up the array's address; make it
+ * before any stream capture.  Runs on the current device, asynchronously on `stream`. */
 int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamma, const double *d_cre,
                             const double *d_cim, int64_t n_zeros, int64_t n_use, int64_t P,
                             const uint64_t *d_v_int, const uint64_t *d_v_frac, const double *d_delta,
@@ -121,9 +122,13 @@ int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamma, const do
  * A plan fixes n_groups groups; group g is the next counts[g] candidates of the candidate
  * array, evaluated at (ks[g], Ts[g]).  Per group the zeros below T are split at a boundary
  * n_heavy chosen so that the a-priori worst-case error bound stays <= tol: the first n_heavy
- * zeros are summed in FP64 (64-bit phase, FP64 polynomials), the rest with a 32-bit phase,
- * MUFU sine/cosine and FP32 accumulation with two-sum compensated partials.  All groups run
- * in one persistent kernel; mb_plan_run replays a captured CUDA graph.
+ * zeros (the heavy tier) are summed in FP64 (64-bit phase, table sine/cosine with FP64
+ * polynomials), the rest (the light tier) with a 32-bit phase, MUFU sine/cosine and FP32
+ * accumulators that are added into FP64 partial sums every 16 terms.  Each tier is one kernel
+ * over the work items of every group: the heavy kernel is persistent (two CTAs per SM pull items
+ * from a counter) and runs on a second stream concurrently with the light kernel (one CTA per
+ * item); a deterministic reduction adds the partial sums.  mb_plan_run replays a captured CUDA
+ * graph of the whole sequence.
  * Replaces the candidate scoring loops of search/eval_tech1_600k.py:201-273,
  * search/eval_tech2_hdrop_600k.py:127-201 and search/eval_sub35_candidates.py:64-138 (which
  * call compute_peak_AB + polish_peaks_with_weights per weight vector), and the k-scan of
@@ -199,6 +204,19 @@ int mb_plan_tier_terms(const mb_plan *p, double *heavy_terms, double *light_term
 /* Measured full-rate instruction issue throughput of `device` (FFMA chains), in thread
  * instructions per second: the peak against which the ALU-bound kernels are reported. */
 int mb_calibrate_issue(int device, double *thread_inst_per_s);
+/* Measured full-rate throughput of `device`'s FMA pipe (FFMA), XU pipe (MUFU sin/cos) and FP64
+ * pipe (DFMA), in thread operations per second (each output nullable): the pipe peaks against
+ * which the tier kernels' algorithmic work is reported.  No reference counterpart. */
+int mb_calibrate_pipes(int device, double *ffma_per_s, double *mufu_per_s, double *dfma_per_s);
+/* Per-kernel timing hook: with n_slots > 0, every later mb_plan_run_dev / mb_plan_run_tiers_dev
+ * records CUDA events around its light-tier launch (on the caller's stream) and its heavy-tier
+ * launch (on the stream it runs on) into a ring of n_slots slots; 0 turns it off.  The plan's
+ * host-pointer runs (its CUDA graph) record nothing.  No reference counterpart. */
+int mb_plan_kernel_timing(mb_plan *p, int n_slots);
+/* The light and heavy kernel times (ms) of the last min(n, n_slots, runs) timed runs, oldest
+ * first, in light_ms / heavy_ms (-1 where that tier did not run); *n_out = how many.  Waits for
+ * those runs' events. */
+int mb_plan_kernel_times(mb_plan *p, int n, double *light_ms, double *heavy_ms, int *n_out);
 
 /* Batched Newton polish of the offsets: h0 = K2 at the given d_delta; then up to `iters` steps
  * delta -= clamp(K2'/K2'', +-max_step) with K2' = dK2/ddelta, K2'' = d2K2/ddelta2 = dK2/dk from
@@ -250,8 +268,9 @@ int mb_screen(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_f
  * d_v_frac hold P leaves; stage_end and threshold are host arrays as above.  Hits go to d_hits /
  * d_hit_scores (device, at most max_hits, in arbitrary order) and their total to *d_n_hits (device;
  * above max_hits the kept subset is arbitrary); d_scores (device, nullable, P x n_stages) as
- * out_scores.  The zero records are staged in the table's scratch buffer: calls on one table that
- * overlap on the GPU race. */
+ * out_scores.  The zero records are staged in a buffer of the table that only mb_screen_dev uses,
+ * so other calls on the table (on its own stream) cannot disturb a screen in flight; two
+ * mb_screen_dev calls on one table that overlap on the GPU (different streams) race on it. */
 int mb_screen_dev(mb_table *t, int64_t P, const uint64_t *d_v_int, const uint64_t *d_v_frac, double k,
                   uint64_t step_int, uint64_t step_frac, int n_stages, const int64_t *stage_end,
                   const float *threshold, int64_t max_hits, int64_t *d_hits, float *d_hit_scores,

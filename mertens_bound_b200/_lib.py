@@ -53,6 +53,9 @@ SIGNATURES: dict[str, tuple] = {
     "mb_plan_newton_dev": (i32, [vp, vp, vp, vp, i32, f64, vp, vp, vp, vp, vp]),
     "mb_plan_tier_terms": (i32, [vp, f64p, f64p]),
     "mb_calibrate_issue": (i32, [i32, f64p]),
+    "mb_calibrate_pipes": (i32, [i32, f64p, f64p, f64p]),
+    "mb_plan_kernel_timing": (i32, [vp, i32]),
+    "mb_plan_kernel_times": (i32, [vp, i32, vp, vp, C.POINTER(i32)]),
     "mb_k2_plain_noalloc_dev": (i32, [vp, vp, vp, vp, i64, i64, i64, vp, vp, vp, f64, vp, vp, vp, vp]),
     "mb_k2_certified": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
     "mb_k2_certified_range": (i32, [vp, i64, vp, vp, vp, f64, f64, i64, i64, vp, vp, vp, vp]),

@@ -380,7 +380,7 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
 // tiers: bit 0 runs the heavy tier, bit 1 the light tier (3 = the full evaluation; a single
 // tier is used to time one kernel on its own -- the result then lacks the other tier).
 int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
-                double *d_dk, cudaStream_t s, int tiers) {
+                double *d_dk, cudaStream_t s, int tiers, const TierEvents *ev) {
     const TabView tv = view(t);
     const bool heavy = (tiers & 1) && pd.n_heavy > 0;
     const bool light = (tiers & 2) && pd.n_light > 0;
@@ -394,12 +394,18 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
             MB_CUDA(cudaStreamWaitEvent(t.side, t.ev_fork, 0));
         }
         MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), hs));
+        if (ev) MB_CUDA(cudaEventRecord(ev->heavy0, hs));
         k2_heavy_kernel<<<pd.heavy_grid, FAST_THREADS, 0, hs>>>(tv, c, pd.items, pd.n_heavy, pd.groups,
                                                                 pd.counter, pd.partial);
         MB_CUDA(cudaGetLastError());
+        if (ev) MB_CUDA(cudaEventRecord(ev->heavy1, hs));
         if (fork) MB_CUDA(cudaEventRecord(t.ev_join, t.side));
     }
-    if (light) MB_TRY(launch_light(tv, pd, c, s));
+    if (light) {
+        if (ev) MB_CUDA(cudaEventRecord(ev->light0, s));
+        MB_TRY(launch_light(tv, pd, c, s));
+        if (ev) MB_CUDA(cudaEventRecord(ev->light1, s));
+    }
     if (fork) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
     fast_reduce_kernel<<<(unsigned)((c.P * 32 + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
                                                                      d_val, d_dd, d_dk);
@@ -454,6 +460,85 @@ int calibrate_issue(int device, double *thread_inst_per_s) {
     }
     *thread_inst_per_s = (double)grid * 256 * iters * 8 / (best * 1e-3);
     return MB_OK;
+}
+
+// Pipe calibration: eight independent dependency chains per thread of one operation, enough warps
+// to fill every scheduler; the rate is thread operations per second.
+__global__ void __launch_bounds__(256) mufu_calibration_kernel(int iters, float *sink) {
+    float f[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i] = 0.25f + 1e-3f * (threadIdx.x + i);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+            asm volatile("sin.approx.f32 %0, %0;" : "+f"(f[i]));
+            asm volatile("cos.approx.f32 %0, %0;" : "+f"(f[i + 1]));
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += f[i];
+    if (s == 123.25f) sink[0] = s;
+}
+
+__global__ void __launch_bounds__(256) dfma_calibration_kernel(int iters, float *sink) {
+    double f[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i] = 1.0 + 1e-3 * (threadIdx.x + i);
+    const double a = 0.9999999999, b = 1e-10;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(f[i]) : "d"(a), "d"(b));
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += f[i];
+    if (s == 123.25) sink[0] = (float)s;
+}
+
+namespace {
+// Best of three timed launches (after one short warm-up) of kern(iters), in thread ops per second
+// (8 chains of `iters` operations per thread).
+template <typename K>
+int time_chains(K kern, unsigned grid, int iters, float *sink, double *rate) {
+    cudaEvent_t e0, e1;
+    MB_CUDA(cudaEventCreate(&e0));
+    MB_CUDA(cudaEventCreate(&e1));
+    kern<<<grid, 256>>>(64, sink);
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+        cudaEventRecord(e0);
+        kern<<<grid, 256>>>(iters, sink);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) {
+        set_error("calibration: %s", cudaGetErrorString(e));
+        return MB_ERR_CUDA;
+    }
+    *rate = (double)grid * 256 * iters * 8 / (best * 1e-3);
+    return MB_OK;
+}
+}  // namespace
+
+int calibrate_pipes(int device, double *ffma_per_s, double *mufu_per_s, double *dfma_per_s) {
+    int sms = 148;
+    MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    float *sink = nullptr;
+    MB_CUDA(cudaMalloc(&sink, sizeof(float)));
+    const unsigned grid = (unsigned)sms * 8;
+    int st = MB_OK;
+    if (ffma_per_s) st = time_chains(issue_calibration_kernel, grid, 8192, sink, ffma_per_s);
+    if (st == MB_OK && mufu_per_s) st = time_chains(mufu_calibration_kernel, grid, 2048, sink, mufu_per_s);
+    if (st == MB_OK && dfma_per_s) st = time_chains(dfma_calibration_kernel, grid, 4096, sink, dfma_per_s);
+    cudaFree(sink);
+    return st;
 }
 
 int heavy_grid_size(int device, unsigned *grid) {

@@ -59,9 +59,19 @@ constexpr double EPS_LIGHT = 2.2e-6;
 constexpr double FUSED_PHASE_GAMMA = 6.283185307179586 * 524287.0;
 constexpr double EPS_HEAVY = 2.0e-13;
 
+// CUDA events recorded around the tier launches of one run (the per-kernel timing hook of
+// mb_plan_kernel_timing): light0/light1 on the launching stream, heavy0/heavy1 on the stream the
+// heavy tier runs on.
+struct TierEvents {
+    cudaEvent_t light0 = nullptr, light1 = nullptr, heavy0 = nullptr, heavy1 = nullptr;
+};
+
 int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
-                double *d_dk, cudaStream_t s, int tiers = 3);
+                double *d_dk, cudaStream_t s, int tiers = 3, const TierEvents *ev = nullptr);
 int heavy_grid_size(int device, unsigned *grid);
 int calibrate_issue(int device, double *thread_inst_per_s);
+// Measured full-rate throughput of the three pipes the tier kernels use, in thread operations
+// per second: FFMA (FMA pipe), MUFU sin/cos (XU pipe), DFMA (FP64 pipe).
+int calibrate_pipes(int device, double *ffma_per_s, double *mufu_per_s, double *dfma_per_s);
 
 }  // namespace mb

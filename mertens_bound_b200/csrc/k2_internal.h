@@ -69,8 +69,10 @@ struct Table {
     cudaStream_t side = nullptr;      // second stream: heavy tier beside the light tier
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // grow-only scratch owned by the table: `io` stages candidates and results of host-pointer
-    // calls, `work` holds per-chunk partial sums.  Calls on one table must not overlap on the GPU.
-    DevBuf io, work;
+    // calls, `work` holds per-chunk partial sums, `screen` the zero records of mb_screen_dev
+    // (which runs on the caller's stream, so it shares no buffer with calls on `stream`).  Calls
+    // on one table that use the same buffer must not overlap on the GPU.
+    DevBuf io, work, screen;
     int n_plans = 0;                  // live plans on this table (it cannot be destroyed under them)
 
     int64_t count_below(double T) const;

@@ -251,7 +251,9 @@ int launch_plain(Table &t, CandView c, int64_t n_use, double k, double *d_val, d
 // All calls on a device share the array: calls that overlap on the GPU (different streams,
 // host threads) race on it.  A call overwrites every slot it later reads, so no earlier
 // contents leak into a result.  The first call on a device looks up the array's device
-// address (cudaGetSymbolAddress); make that first call before any stream capture.
+// address (cudaGetSymbolAddress); make that first call before any stream capture.  The address
+// is kept with the device's current context and looked up again when the context changes (after
+// a cudaDeviceReset the array lives at a new address in the new primary context).
 namespace {
 
 constexpr int64_t NOALLOC_PARTIAL_DOUBLES = (int64_t)1 << 20;
@@ -259,9 +261,28 @@ static __device__ __align__(256) double g_noalloc_partial[NOALLOC_PARTIAL_DOUBLE
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+void *g_noalloc_ctx[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_noalloc_mu;
 
-// Device address of the array on the current device (set up once per device).
+// The current context handle through the driver's cuCtxGetCurrent (fetched with
+// cudaGetDriverEntryPoint, so the library does not link the driver library itself); null if it
+// cannot be had.
+void *current_context() {
+    typedef int (*ctx_fn)(void **);
+    static ctx_fn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (ctx_fn)f;
+    }();
+    void *ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
+// Device address of the array on the current device (set up once per device and context).
 int noalloc_scratch(double **out) {
     int dev = -1;
     MB_CUDA(cudaGetDevice(&dev));
@@ -269,8 +290,9 @@ int noalloc_scratch(double **out) {
         mb::set_error("no-allocation scratch: device %d out of range", dev);
         return MB_ERR_ARG;
     }
+    void *ctx = current_context();
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev] || ctx != g_noalloc_ctx[dev]) {
         double *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_partial);
         if (e != cudaSuccess || p == nullptr) {
@@ -279,6 +301,7 @@ int noalloc_scratch(double **out) {
             return MB_ERR_CUDA;
         }
         g_noalloc_addr[dev] = p;
+        g_noalloc_ctx[dev] = current_context();     // current now, if it was not on entry
     }
     *out = g_noalloc_addr[dev];
     return MB_OK;
@@ -292,9 +315,12 @@ extern "C" int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamm
                                        const double *d_delta, double k, double *d_val, double *d_dd,
                                        double *d_dk, void *stream) {
     using namespace mb;
-    MB_CHECK_ARG(P >= 0 && P * 3 <= NOALLOC_PARTIAL_DOUBLES,
-                 "mb_k2_plain_noalloc_dev: P=%lld exceeds the fixed scratch (at most %lld candidates)",
-                 (long long)P, (long long)(NOALLOC_PARTIAL_DOUBLES / 3));
+    MB_CHECK_ARG(P >= 0, "mb_k2_plain_noalloc_dev: P=%lld", (long long)P);
+    if (P * 3 > NOALLOC_PARTIAL_DOUBLES) {
+        set_error("mb_k2_plain_noalloc_dev: P=%lld exceeds the fixed scratch (at most %lld candidates)",
+                  (long long)P, (long long)(NOALLOC_PARTIAL_DOUBLES / 3));
+        return MB_ERR_CAPACITY;
+    }
     MB_CHECK_ARG(d_g && d_gamma && d_cre && d_cim && d_v_int && d_v_frac && d_val && d_dd && d_dk,
                  "mb_k2_plain_noalloc_dev: null argument");
     MB_CHECK_ARG(n_zeros >= 1 && n_use >= 0 && n_use <= n_zeros, "mb_k2_plain_noalloc_dev: n_use=%lld n_zeros=%lld",

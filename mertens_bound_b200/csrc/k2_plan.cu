@@ -42,9 +42,25 @@ struct mb_plan {
     cudaGraphExec_t graph = nullptr;
     DevBuf newton_buf;             // Newton polish: starting point, its gradients, stop flags
     DevBuf flush_buf;              // mb_plan_time: written between timed runs to empty the L2
+    // per-kernel timing hook (mb_plan_kernel_timing): a ring of event sets, one per device run
+    std::vector<TierEvents> tev;
+    std::vector<signed char> tev_tiers;   // tiers each slot's run launched (bit 0 heavy, 1 light)
+    long long tev_runs = 0;
+    void release_events() {
+        for (TierEvents &e : tev) {
+            cudaEventDestroy(e.light0);
+            cudaEventDestroy(e.light1);
+            cudaEventDestroy(e.heavy0);
+            cudaEventDestroy(e.heavy1);
+        }
+        tev.clear();
+        tev_tiers.clear();
+        tev_runs = 0;
+    }
     ~mb_plan() {
         newton_buf.release();
         flush_buf.release();
+        release_events();
     }
 };
 
@@ -248,6 +264,21 @@ int upload(mb_plan *p) {
 int plan_run_dev(mb_plan *p, const uint64_t *vi, const uint64_t *vf, const double *delta, double *val,
                  double *dd, double *dk, cudaStream_t s) {
     return launch_fast(*p->table, p->dev, CandView{vi, vf, delta, p->P}, val, dd, dk, s);
+}
+
+// A device-pointer run that records the timing hook's events when it is on (never inside the
+// plan's own graph capture: ensure_io calls plan_run_dev directly).
+int plan_run_timed(mb_plan *p, int tiers, const uint64_t *vi, const uint64_t *vf, const double *delta,
+                   double *val, double *dd, double *dk, cudaStream_t s) {
+    const TierEvents *ev = nullptr;
+    if (!p->tev.empty()) {
+        const size_t slot = (size_t)(p->tev_runs % (long long)p->tev.size());
+        ev = &p->tev[slot];
+        p->tev_tiers[slot] = (signed char)(((tiers & 1) && p->dev.n_heavy > 0 ? 1 : 0) |
+                                           ((tiers & 2) && p->dev.n_light > 0 ? 2 : 0));
+        ++p->tev_runs;
+    }
+    return launch_fast(*p->table, p->dev, CandView{vi, vf, delta, p->P}, val, dd, dk, s, tiers, ev);
 }
 
 int ensure_io(mb_plan *p) {
@@ -550,7 +581,7 @@ extern "C" int mb_plan_run_dev(mb_plan *p, const uint64_t *d_vi, const uint64_t 
                                void *stream) {
     MB_CHECK_ARG(p && d_vi && d_vf && d_val && d_dd && d_dk, "mb_plan_run_dev: null argument");
     MB_TRY(device_guard(p->table->device));
-    return plan_run_dev(p, d_vi, d_vf, d_delta, d_val, d_dd, d_dk, (cudaStream_t)stream);
+    return plan_run_timed(p, 3, d_vi, d_vf, d_delta, d_val, d_dd, d_dk, (cudaStream_t)stream);
 }
 
 extern "C" int mb_plan_run_tiers_dev(mb_plan *p, int tiers, const uint64_t *d_vi, const uint64_t *d_vf,
@@ -559,8 +590,57 @@ extern "C" int mb_plan_run_tiers_dev(mb_plan *p, int tiers, const uint64_t *d_vi
     MB_CHECK_ARG(p && d_vi && d_vf && d_val && d_dd && d_dk, "mb_plan_run_tiers_dev: null argument");
     MB_CHECK_ARG(tiers >= 1 && tiers <= 3, "mb_plan_run_tiers_dev: tiers=%d (1 heavy, 2 light, 3 both)", tiers);
     MB_TRY(device_guard(p->table->device));
-    return launch_fast(*p->table, p->dev, CandView{d_vi, d_vf, d_delta, p->P}, d_val, d_dd, d_dk,
-                       (cudaStream_t)stream, tiers);
+    return plan_run_timed(p, tiers, d_vi, d_vf, d_delta, d_val, d_dd, d_dk, (cudaStream_t)stream);
+}
+
+extern "C" int mb_plan_kernel_timing(mb_plan *p, int n_slots) {
+    MB_CHECK_ARG(p && n_slots >= 0 && n_slots <= 100000, "mb_plan_kernel_timing: bad argument (n_slots=%d)",
+                 n_slots);
+    MB_TRY(device_guard(p->table->device));
+    // runs still in flight may record the old events: wait for them before destroying any
+    if (!p->tev.empty()) MB_CUDA(cudaDeviceSynchronize());
+    p->release_events();
+    p->tev.resize((size_t)n_slots);
+    p->tev_tiers.assign((size_t)n_slots, 0);
+    for (TierEvents &e : p->tev) {
+        cudaError_t r = cudaEventCreate(&e.light0);
+        if (r == cudaSuccess) r = cudaEventCreate(&e.light1);
+        if (r == cudaSuccess) r = cudaEventCreate(&e.heavy0);
+        if (r == cudaSuccess) r = cudaEventCreate(&e.heavy1);
+        if (r != cudaSuccess) {
+            p->release_events();
+            set_error("mb_plan_kernel_timing: %s", cudaGetErrorString(r));
+            return MB_ERR_CUDA;
+        }
+    }
+    return MB_OK;
+}
+
+extern "C" int mb_plan_kernel_times(mb_plan *p, int n, double *light_ms, double *heavy_ms, int *n_out) {
+    MB_CHECK_ARG(p && n >= 0 && n_out, "mb_plan_kernel_times: bad argument");
+    MB_CHECK_ARG(n == 0 || (light_ms && heavy_ms), "mb_plan_kernel_times: null output");
+    MB_TRY(device_guard(p->table->device));
+    const long long slots = (long long)p->tev.size();
+    const long long have = std::min<long long>(std::min<long long>(p->tev_runs, slots), n);
+    *n_out = (int)have;
+    for (long long i = 0; i < have; ++i) {
+        const long long run = p->tev_runs - have + i;
+        const size_t slot = (size_t)(run % slots);
+        const TierEvents &e = p->tev[slot];
+        float ms = -1.f;
+        light_ms[i] = heavy_ms[i] = -1.0;
+        if (p->tev_tiers[slot] & 2) {
+            MB_CUDA(cudaEventSynchronize(e.light1));
+            MB_CUDA(cudaEventElapsedTime(&ms, e.light0, e.light1));
+            light_ms[i] = ms;
+        }
+        if (p->tev_tiers[slot] & 1) {
+            MB_CUDA(cudaEventSynchronize(e.heavy1));
+            MB_CUDA(cudaEventElapsedTime(&ms, e.heavy0, e.heavy1));
+            heavy_ms[i] = ms;
+        }
+    }
+    return MB_OK;
 }
 
 extern "C" int mb_plan_tier_terms(const mb_plan *p, double *heavy_terms, double *light_terms) {
@@ -579,6 +659,12 @@ extern "C" int mb_calibrate_issue(int device, double *thread_inst_per_s) {
     MB_CHECK_ARG(thread_inst_per_s, "mb_calibrate_issue: null output");
     MB_TRY(device_guard(device));
     return calibrate_issue(device, thread_inst_per_s);
+}
+
+extern "C" int mb_calibrate_pipes(int device, double *ffma_per_s, double *mufu_per_s, double *dfma_per_s) {
+    MB_CHECK_ARG(ffma_per_s || mufu_per_s || dfma_per_s, "mb_calibrate_pipes: no output");
+    MB_TRY(device_guard(device));
+    return calibrate_pipes(device, ffma_per_s, mufu_per_s, dfma_per_s);
 }
 
 extern "C" int mb_plan_run(mb_plan *p, const uint64_t *vi, const uint64_t *vf, const double *delta,

@@ -250,8 +250,8 @@ extern "C" int mb_screen_dev(mb_table *h, int64_t P, const uint64_t *d_v_int, co
         return MB_OK;
     }
     const int nz = sa.stage_end[n_stages - 1];
-    MB_TRY(t.work.ensure(nz * sizeof(ZScreen)));
-    MB_TRY(launch_screen(t, P, d_v_int, d_v_frac, k, step_int, step_frac, sa, (ZScreen *)t.work.p, max_hits,
+    MB_TRY(t.screen.ensure(nz * sizeof(ZScreen)));
+    MB_TRY(launch_screen(t, P, d_v_int, d_v_frac, k, step_int, step_frac, sa, (ZScreen *)t.screen.p, max_hits,
                          d_n_hits, d_hits, d_hit_scores, d_scores, st));
     return MB_OK;
 }

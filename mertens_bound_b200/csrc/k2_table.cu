@@ -80,6 +80,7 @@ static void free_table(Table &t) {
     cudaFree(t.d_psi);
     t.io.release();
     t.work.release();
+    t.screen.release();
     for (double *w : t.d_weights) cudaFree(w);
     if (t.ev_fork) cudaEventDestroy(t.ev_fork);
     if (t.ev_join) cudaEventDestroy(t.ev_join);

@@ -30,6 +30,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 #include <quadmath.h>
 
@@ -73,11 +74,26 @@ static inline __float128 G_quad(const uint64_t *g) {
  *   w = exp(-k gam^2) (or wts[j] when wts is given: the search drivers' other weight
  *   kernels, search/eval_tech1_600k.py:243-249), gam = 2pi G (exact G, not the FP64 gamma).
  * Zeros j < n_use are summed (the caller applies the cutoff gamma < T).
+ * gam and w depend on the zero only, so they are formed once per zero (in binary128, the same
+ * operations as per term) and shared by every candidate.
  * Each output is returned as a double pair (hi, lo) with hi + lo = the binary128 sum
  * rounded to ~106 bits, so tests can see errors far below one FP64 ulp. */
 void orc_k2_quad_w(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
                    int64_t n_use, const uint64_t *G3, const double *c_re, const double *c_im,
                    double k, const double *wts, double *out /* P x 6: val hi,lo, dd hi,lo, dk hi,lo */) {
+    __float128 *gq = (__float128 *)malloc(sizeof(__float128) * (size_t)(n_use > 0 ? n_use : 1));
+    __float128 *wq = (__float128 *)malloc(sizeof(__float128) * (size_t)(n_use > 0 ? n_use : 1));
+    if (!gq || !wq) {
+        free(gq);
+        free(wq);
+        for (int64_t i = 0; i < 6 * P; ++i) out[i] = NAN;
+        return;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < n_use; ++j) {
+        gq[j] = Q_2PI * G_quad(&G3[3 * j]);
+        wq[j] = wts ? (__float128)wts[j] : expq(-(__float128)k * gq[j] * gq[j]);
+    }
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t p = 0; p < P; ++p) {
         __float128 sv = 0, sd = 0, sk = 0;
@@ -85,13 +101,11 @@ void orc_k2_quad_w(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, con
         for (int64_t j = 0; j < n_use; ++j) {
             uint64_t hi, lo;
             phase128(v_int[p], v_frac[p], G3[3 * j], G3[3 * j + 1], G3[3 * j + 2], &hi, &lo);
-            __float128 G = G_quad(&G3[3 * j]);
-            __float128 gam = Q_2PI * G;
+            const __float128 gam = gq[j], w = wq[j];
             __float128 fr = ldexpq((__float128)hi, -64) + ldexpq((__float128)lo, -128);
             __float128 th = Q_2PI * fr + gam * dq;
             __float128 s, c;
             sincosq(th, &s, &c);
-            __float128 w = wts ? (__float128)wts[j] : expq(-(__float128)k * gam * gam);
             __float128 re = (__float128)c_re[j] * c - (__float128)c_im[j] * s;
             __float128 im = (__float128)c_re[j] * s + (__float128)c_im[j] * c;
             sv += w * re;
@@ -105,6 +119,8 @@ void orc_k2_quad_w(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, con
             out[6 * p + 2 * i + 1] = (double)(r[i] - (__float128)h);
         }
     }
+    free(gq);
+    free(wq);
 }
 
 void orc_k2_quad(int64_t P, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,

@@ -97,14 +97,17 @@ def small_fixture():
     return out
 
 
-REF_PATH1 = "/root/reference/search/path1_kernel_opt.py"
+# The reference checkout: --ref, or the environment variable MB_REFERENCE_DIR, else a directory
+# named `reference` beside this repository.
+REF_DIR = os.environ.get("MB_REFERENCE_DIR",
+                         os.path.abspath(os.path.join(HERE, "..", "..", "..", "reference")))
 
 
 def reference_path1_functions():
     """polish_single_peak and fast_polish_batch_blas from the reference source, executed in a
     namespace holding only numpy and math."""
     import ast
-    tree = ast.parse(open(REF_PATH1).read())
+    tree = ast.parse(open(os.path.join(REF_DIR, "search", "path1_kernel_opt.py")).read())
     keep = [n for n in tree.body if isinstance(n, ast.FunctionDef)
             and n.name in ("polish_single_peak", "fast_polish_batch_blas")]
     ns = {"np": np, "math": math}
@@ -198,7 +201,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-full-ball", action="store_true")
     ap.add_argument("--workers", type=int, default=os.cpu_count())
+    ap.add_argument("--ref", default=None, help="the reference checkout (default: MB_REFERENCE_DIR or "
+                                                "../reference beside the repository)")
     a = ap.parse_args()
+    global REF_DIR
+    if a.ref:
+        REF_DIR = os.path.abspath(a.ref)
     with open(os.path.join(HERE, "small_plain.json"), "w") as f:
         json.dump(small_fixture(), f, indent=1)
     print("wrote small_plain.json", flush=True)
