@@ -184,6 +184,26 @@ def batched_uneven_groups():
     return counts, ks, Ts
 
 
+# The enumerators' screen and hit polish compare absolute scores with fixed thresholds (0.81 ..
+# 0.948).  With the generator's coefficients the first 64 zeros carry sum 2|c| w = 1.08, so random
+# leaves never reach them (the enumerators' leaves come from a lattice search that aligns the
+# phases); a table with c scaled by 3 lets about 9% of random leaves pass the screen and run the
+# polish to its last stage, so both sides of every threshold are exercised.
+ENUM_C_SCALE = 3.0
+
+
+def enumerator_table(n: int = 40_000, seed: int = 1, c_scale: float = ENUM_C_SCALE) -> ZeroTableData:
+    """make_table(n, seed) with every coefficient c multiplied by c_scale."""
+    t = make_table(n, seed=seed)
+    return ZeroTableData(t.G3, t.gamma, t.c_re * c_scale, t.c_im * c_scale, t.seed)
+
+
+def leaves_x(count: int, seed: int) -> list:
+    """x = floor(v 2^30) (Python ints, the enumerators' u128 leaf form) of make_candidates(count, seed)."""
+    c = make_candidates(count, seed=seed)
+    return [(int(a) << 30) | (int(b) >> 34) for a, b in zip(c.v_int, c.v_frac)]
+
+
 # The five workloads (sizes, cutoffs and Gaussian widths) the evaluator is measured on.
 WORKLOADS = {
     "small_plain": dict(n_zeros=10_000, T=math.inf, k=3e-9, P=64, table_seed=1, cand_seed=2),

@@ -17,6 +17,9 @@ Contents
   * Oracle.fast_screen  -- restated ZeroData::fast_screen (search/fast_mertens_enum.cpp:108-142).
   * RefLib              -- binding of _ref/libpath1_eval.so, the reference's own evaluator
                            compiled from search/path1_eval_fast.cpp (see Makefile).
+  * ZeroDataRef         -- binding of _ref/libzerodata_ref.so, the reference enumerator's own
+                           ZeroData (search/fast_mertens_enum.cpp:27-277: load, fast_screen,
+                           polish) behind the harness zerodata_ref.cpp.
 """
 from __future__ import annotations
 
@@ -29,6 +32,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libpath1_eval.so")
+ZD_SO = os.path.join(HERE, "_ref", "libzerodata_ref.so")
 MASK64 = (1 << 64) - 1
 MASK128 = (1 << 128) - 1
 
@@ -312,3 +316,60 @@ class RefLib:
                                          _p(np.ascontiguousarray(gamma[:n])), _p(np.ascontiguousarray(w[:n])),
                                          float(half), int(steps), _p(hu), _p(hp), _p(dp))
         return hu, hp, dp
+
+
+# ------------------------------------------------------------------ the reference's ZeroData
+
+class ZeroDataRef:
+    """The reference enumerator's ZeroData (search/fast_mertens_enum.cpp:27-277), compiled from its
+    source by the Makefile, on a zeros.bin file (at least 15,000 zeros: polish() reads that many).
+    Leaves and hits are x = floor(y 2^30) as u128 (x_lo, x_hi words), as the enumerators hold them."""
+
+    def __init__(self, zeros_bin_path: str):
+        if not os.path.exists(ZD_SO):
+            build()
+        if not os.path.exists(ZD_SO):
+            raise FileNotFoundError(ZD_SO)
+        L = C.CDLL(ZD_SO)
+        L.zd_load.argtypes = [C.c_char_p]
+        L.zd_load.restype = C.c_void_p
+        L.zd_free.argtypes = [C.c_void_p]
+        L.zd_n_zeros.argtypes = [C.c_void_p]
+        L.zd_fast_screen.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.zd_polish.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        self.L = L
+        self.h = L.zd_load(zeros_bin_path.encode())
+        if not self.h:
+            raise OSError(f"ZeroData::load failed on {zeros_bin_path}")
+        if L.zd_n_zeros(self.h) < 15000:
+            self.close()
+            raise ValueError("ZeroData::polish needs at least 15,000 zeros")
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(ZD_SO)
+
+    def fast_screen(self, x_lo, x_hi):
+        x_lo = np.ascontiguousarray(x_lo, dtype=np.uint64)
+        x_hi = np.ascontiguousarray(x_hi, dtype=np.uint64)
+        out = np.zeros(x_lo.shape[0], dtype=np.uint8)
+        self.L.zd_fast_screen(self.h, x_lo.shape[0], _p(x_lo), _p(x_hi), _p(out))
+        return out
+
+    def polish(self, x_lo, x_hi):
+        x_lo = np.ascontiguousarray(x_lo, dtype=np.uint64)
+        x_hi = np.ascontiguousarray(x_hi, dtype=np.uint64)
+        h, dy = np.empty(x_lo.shape[0]), np.empty(x_lo.shape[0])
+        self.L.zd_polish(self.h, x_lo.shape[0], _p(x_lo), _p(x_hi), _p(h), _p(dy))
+        return h, dy
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.zd_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

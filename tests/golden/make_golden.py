@@ -12,6 +12,10 @@ small_plain.json    64 candidates x 10,000 synthetic zeros (table seed 1, candid
                       * mpmath interval balls of K2 and of dK2/ddelta, dK2/dk for 4 candidates
                         (220 bits);
                       * exact phases floor(frac(v G) 2^128) for 16 (candidate, zero) pairs.
+zerodata_ref.json   the reference enumerator's own ZeroData (search/fast_mertens_enum.cpp, compiled
+                    by oracle/Makefile through oracle/zerodata_ref.cpp) on synth.enumerator_table()
+                    (40,000 zeros, c scaled by 3): fast_screen decisions of 16,384 leaves and
+                    polish (h, dy) of 48 hits (--only zerodata writes just this one).
 peak2_full_ball.json the interval ball of K2 at the reference's Peak2 point over all 2,325,572
                     synthetic zeros below 1.3e6 (table seed 1), k = 1.5e-10, as exact rational
                     endpoints (mpmath iv at 220 bits, summed in 64 worker processes' chunks),
@@ -197,16 +201,60 @@ def full_ball_fixture(workers: int):
             "seconds": round(time.time() - t0, 1)}
 
 
+def zerodata_fixture():
+    """The reference enumerator's own ZeroData (search/fast_mertens_enum.cpp:27-277, compiled from
+    its source into oracle/_ref/libzerodata_ref.so) on synth.enumerator_table() written as a
+    zeros.bin: fast_screen decisions of 16,384 random leaves and polish (h, dy) of 48 hits (the 32
+    leaves of largest |h| among the first 4,096, which run all five stages, and 16 others)."""
+    import tempfile
+    from mertens_bound_b200 import formats
+    from oracle.oracle import MASK64, ZeroDataRef
+
+    t = synth.enumerator_table()
+    f = formats.reference_fields(t, exact_psi=True)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "zeros.bin")
+        formats.write_zeros_bin(path, f)
+        Z = ZeroDataRef(path)
+        x = synth.leaves_x(16384, seed=21)
+        x_lo = np.array([v & MASK64 for v in x], np.uint64)
+        x_hi = np.array([v >> 64 for v in x], np.uint64)
+        passed = Z.fast_screen(x_lo, x_hi)
+        h, dy = Z.polish(x_lo[:4096], x_hi[:4096])
+        deep = np.argsort(-np.abs(h), kind="stable")[:32]
+        rest = np.setdiff1d(np.arange(4096), deep)
+        other = np.random.default_rng(22).choice(rest, 16, replace=False)
+        sel = np.concatenate([np.sort(deep), np.sort(other)])
+        Z.close()
+    xs = np.array([[v & MASK64, v >> 64] for v in x], np.uint64)
+    return {"table": {"n": t.n, "seed": 1, "c_scale": synth.ENUM_C_SCALE, "sha256": table_sha(t)},
+            "zeros_bin": "formats.reference_fields(exact_psi=True) -> formats.write_zeros_bin "
+                         "(two_astar = 2|c| exp(-3e-9 gamma^2))",
+            "leaves": {"count": 16384, "seed": 21, "form": "x = floor(v 2^30) of synth.make_candidates",
+                       "sha256": hashlib.sha256(xs.tobytes()).hexdigest()},
+            "screen_pass_packbits_hex": np.packbits(passed).tobytes().hex(), "screen_passed": int(passed.sum()),
+            "polish": [{"leaf": int(i), "x": str(x[i]), "h": float(h[i]), "dy": float(dy[i])} for i in sel],
+            "source": "search/fast_mertens_enum.cpp ZeroData::load/fast_screen/polish via oracle/zerodata_ref.cpp"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-full-ball", action="store_true")
     ap.add_argument("--workers", type=int, default=os.cpu_count())
+    ap.add_argument("--only", choices=["zerodata"], default=None,
+                    help="write only this fixture (zerodata: zerodata_ref.json, needs oracle/_ref built from "
+                         "the reference source)")
     ap.add_argument("--ref", default=None, help="the reference checkout (default: MB_REFERENCE_DIR or "
                                                 "../reference beside the repository)")
     a = ap.parse_args()
     global REF_DIR
     if a.ref:
         REF_DIR = os.path.abspath(a.ref)
+    if a.only == "zerodata":
+        with open(os.path.join(HERE, "zerodata_ref.json"), "w") as f:
+            json.dump(zerodata_fixture(), f, indent=1)
+        print("wrote zerodata_ref.json", flush=True)
+        return
     with open(os.path.join(HERE, "small_plain.json"), "w") as f:
         json.dump(small_fixture(), f, indent=1)
     print("wrote small_plain.json", flush=True)
