@@ -101,6 +101,17 @@ int mb_k2_certified_range(mb_table *t, int64_t P, const uint64_t *v_int, const u
                           const double *v_rad, double k_lo, double k_hi, int64_t j0, int64_t j1,
                           const double *term_rad, double *out_lo, double *out_hi, double *out_abs_hi);
 
+/* Certified intervals of K2 and of both derivatives over the zeros [j0, j1), k anywhere in
+ * [k_lo, k_hi]: out_lo / out_hi hold 3P entries, rows K2, dK2/ddelta (= dK2/dv =
+ * -2 sum w gamma Im(c e^{i gamma v})) and dK2/dk (= -2 sum w gamma^2 Re(c e^{i gamma v})), each
+ * enclosed rigorously from the same directed-rounding sine/cosine, weight and gamma intervals as
+ * mb_k2_certified_range; v_rad and term_rad widen the derivative terms by the extra factors
+ * gamma_hi and gamma_hi^2.  The derivatives of certification/certify_K2.py:116-121's term (that
+ * script encloses only the value): the interval check of the gradients the chosen form returns. */
+int mb_k2_certified_grad_range(mb_table *t, int64_t P, const uint64_t *v_int, const uint64_t *v_frac,
+                               const double *v_rad, double k_lo, double k_hi, int64_t j0, int64_t j1,
+                               const double *term_rad, double *out_lo, double *out_hi);
+
 /* Plain FP64 K2 for callers that cannot allocate device memory: no counterpart in the
  * reference (its evaluator is host code).  Callers in a host callback, inside a fixed memory
  * budget or in a runtime that owns every allocation cannot call cudaMalloc; this entry point

@@ -59,6 +59,7 @@ SIGNATURES: dict[str, tuple] = {
     "mb_k2_plain_noalloc_dev": (i32, [vp, vp, vp, vp, i64, i64, i64, vp, vp, vp, f64, vp, vp, vp, vp]),
     "mb_k2_certified": (i32, [vp, i64, vp, vp, vp, f64, f64, vp, vp, vp, vp]),
     "mb_k2_certified_range": (i32, [vp, i64, vp, vp, vp, f64, f64, i64, i64, vp, vp, vp, vp]),
+    "mb_k2_certified_grad_range": (i32, [vp, i64, vp, vp, vp, f64, f64, i64, i64, vp, vp, vp]),
     "mb_grid_scan": (i32, [vp, i64, vp, vp, f64, f64, C.c_uint64, C.c_uint64, i64, i64, vp]),
     "mb_hit_scan": (i32, [vp, i64, vp, vp, f64, i64, C.c_uint64, C.c_uint64, i64, i64, vp]),
     "mb_exact_AB": (i32, [vp, i64, vp, vp, vp, i64, vp, vp]),

@@ -256,6 +256,27 @@ def k2_certified(table: ZeroTable, cands, k: float, T: float = math.inf, v_rad=N
     return lo, hi, ab
 
 
+def k2_certified_grad(table: ZeroTable, cands, k: float, T: float = math.inf, v_rad=None, term_rad=None,
+                      k_hi: float | None = None):
+    """Rigorous enclosures of K2, dK2/ddelta and dK2/dk at v = v_int + v_frac 2^-64 (widened by
+    v_rad), for k in [k, k_hi] (k_hi defaults to k): returns lo, hi of shape (3, P), rows
+    (K2, dK2/ddelta, dK2/dk)."""
+    vi, vf, d = _cand_arrays(cands)
+    if d is not None and np.any(d != 0):
+        raise ValueError("the certified evaluation takes exact 64.64 points; pass offsets as v_rad")
+    P = vi.shape[0]
+    vr = None if v_rad is None else _f64(np.broadcast_to(v_rad, (P,)))
+    n_use = table.count_below(T)
+    tr = None if term_rad is None else _f64(term_rad)
+    if tr is not None and tr.shape != (n_use,):
+        raise ValueError(f"term_rad must have count_below(T) = {n_use} entries")
+    lo, hi = np.empty((3, P)), np.empty((3, P))
+    check(_lib.lib().mb_k2_certified_grad_range(table.handle, P, ptr(vi), ptr(vf), ptr(vr), float(k),
+                                                float(k if k_hi is None else k_hi), 0, n_use, ptr(tr), ptr(lo),
+                                                ptr(hi)))
+    return lo, hi
+
+
 def k2_fast(table: ZeroTable, cands, k: float, T: float = math.inf, tol: float = 1e-10):
     """Chosen-form K2, dK2/ddelta, dK2/dk and the a-priori error bound (one group)."""
     vi, vf, d = _cand_arrays(cands)

@@ -89,3 +89,38 @@ def test_certified_maximum_batch(table, small_table, oracle):
     assert np.all(lo[idx] <= v) and np.all(v <= hi[idx])
     with pytest.raises(K2Error, match="MB_ERR_ARG"):
         k2.k2_certified(table, synth.make_candidates(65_536, seed=55), 3e-9, T)
+
+
+def test_certified_grad_contains_derivative_balls(table, small_table):
+    """K2, dK2/ddelta and dK2/dk enclosures against the committed 220-bit interval balls of
+    tests/golden/small_plain.json (mpmath iv, the restatement of certify_K2.py's Arb sum and its
+    derivatives), and the K2 row equal to mb_k2_certified's interval."""
+    import json
+    import os
+    from fractions import Fraction
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "small_plain.json")))
+    cd = synth.make_candidates(64, seed=2).subset(np.arange(4))
+    lo, hi = k2.k2_certified_grad(table, cd, fx["k"])
+    vlo, vhi, _ = k2.k2_certified(table, cd, fx["k"])
+    assert np.array_equal(lo[0], vlo) and np.array_equal(hi[0], vhi)
+    for p in range(4):
+        a, b = (Fraction(x) for x in fx["interval_balls_first4"][p])
+        assert Fraction(lo[0, p]) <= a and b <= Fraction(hi[0, p])
+        for row, key in ((1, "dd"), (2, "dk")):
+            a, b = (Fraction(x) for x in fx["derivative_balls_first4"][p][key])
+            assert Fraction(lo[row, p]) <= a and b <= Fraction(hi[row, p]), (p, key)
+            mid = abs(float(a + b) / 2)
+            assert hi[row, p] - lo[row, p] < 1e-10 * mid, (p, key, hi[row, p] - lo[row, p], mid)
+
+
+def test_certified_grad_contains_quad_oracle(table, small_table, oracle):
+    cd = synth.make_candidates(40, seed=56)
+    for k, T in ((3e-9, math.inf), (1.5e-10, 30000.0)):
+        lo, hi = k2.k2_certified_grad(table, cd, k, T)
+        ohi, olo = oracle.k2(cd, small_table, k, small_table.count_below(T))
+        for row in range(3):
+            v = ohi[:, row] + olo[:, row]
+            assert np.all(lo[row] <= v) and np.all(v <= hi[row]), row
+        # radii widen every row
+        lo2, hi2 = k2.k2_certified_grad(table, cd, k, T, v_rad=1e-12)
+        assert np.all(lo2 <= lo) and np.all(hi2 >= hi) and np.all(hi2 - lo2 > hi - lo)

@@ -142,6 +142,23 @@ def test_newton_polish_derivatives_vs_oracle(big, oracle):
         _, dd, dk = ev.evaluate(vi, vf, d, K)
         got[2] = dk.cpu().numpy()[sel]
         _check_bounds(plan, 0, got, ohi)
+        # the certified enclosures of K2 and both derivatives at the same 16 points (delta folded
+        # into the 64.64 base, rounded to nearest 2^-64 as the plan does; v_rad covers the rounding):
+        # each autograd output lies within its a-priori bound of its interval
+        from fractions import Fraction
+        pts = []
+        for i in sel:
+            x = (int(cands.v_int[i]) << 64) + int(cands.v_frac[i]) + Fraction(float(cands.delta[i])) * 2 ** 64
+            pts.append(int(x + Fraction(1, 2)) if x >= 0 else int(x - Fraction(1, 2)))
+        cb = synth.Candidates(np.array([x >> 64 for x in pts], np.uint64),
+                              np.array([x & ((1 << 64) - 1) for x in pts], np.uint64), np.zeros(len(sel)))
+        clo, chi = k2.k2_certified_grad(t, cb, K, T, v_rad=2.0 ** -64)
+        gi = plan.group_info(0)
+        for q, key in ((0, "err_bound"), (1, "err_bound_dd"), (2, "err_bound_dk")):
+            dist = np.maximum(np.maximum(clo[q] - got[q], got[q] - chi[q]), 0.0)
+            assert np.max(dist) <= gi[key], (key, np.max(dist), gi[key])
+            ulp = np.spacing(np.abs(ohi[:, q]))               # the oracle's value rounded to FP64
+            assert np.all(clo[q] - ulp <= ohi[:, q]) and np.all(ohi[:, q] <= chi[q] + ulp), key
         # k.grad = sum_p dK2_p/dk
         gk = float(kk.grad.item())
         assert abs(gk - float(dk.sum().item())) <= 1e-12 * float(dk.abs().sum().item())
