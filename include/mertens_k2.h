@@ -185,6 +185,13 @@ int mb_plan_set_shape(mb_plan *p, int g, int cpt, int nzw, int64_t heavy_chunk, 
  * thread (2, 3, 4), extra doublings of each group's warp split (0..3), and a scale of the
  * automatic work-item size (0.125..8).  Replaces per-group overrides. */
 int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, double chunk_scale);
+/* How the two tiers run: 0 (the default) launches the persistent heavy kernel on a second stream
+ * concurrently with the light kernel (one CTA per item); 1 runs every item of both tiers in one
+ * persistent kernel (two CTAs per SM pulling heavy items first, then light items, from one
+ * counter).  The results are the same bits either way.  The autotuner tries both.  No reference
+ * counterpart. */
+int mb_plan_set_schedule(mb_plan *p, int schedule);
+int mb_plan_schedule(const mb_plan *p, int *schedule);
 /* Restrict every group to the zeros [j0, j1) of its [0, count_below(T)): one shard of a
  * zero-range split across GPUs; the shards' results add up to the whole sum (tier boundaries and
  * error bounds are those of the whole sum).  No reference counterpart (the reference shards zero

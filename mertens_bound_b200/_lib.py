@@ -43,6 +43,8 @@ SIGNATURES: dict[str, tuple] = {
     "mb_plan_info": (i32, [vp, i64p, f64p, C.POINTER(i32)]),
     "mb_plan_light_form": (i32, [vp, C.POINTER(i32)]),
     "mb_plan_configure": (i32, [vp, i32, i32, f64]),
+    "mb_plan_set_schedule": (i32, [vp, i32]),
+    "mb_plan_schedule": (i32, [vp, C.POINTER(i32)]),
     "mb_plan_set_zero_range": (i32, [vp, i64, i64]),
     "mb_plan_time": (i32, [vp, i32, f64p]),
     "mb_plan_group_info": (i32, [vp, i32, i64p, i64p, f64p, f64p]),

@@ -1,10 +1,12 @@
 """Autotuner for the chosen-form plans.
 
-The search space is the plan-wide tile configuration (mb_plan_configure):
+The search space is the plan-wide tile configuration (mb_plan_configure) under each schedule
+(mb_plan_set_schedule):
   light_cpt    candidates per thread in the light kernel: 2, 3, 4 (register budget 64/80/128,
                i.e. 4/3/2 CTAs per SM)
   nzw_shift    extra doublings of the warps that split one candidate set's zeros
   chunk_scale  work-item size relative to the automatic choice
+  schedule     0: the two tier kernels concurrently, 1: one persistent kernel for both tiers
 Every configuration is timed on the device (median of `reps` runs, synthetic candidates) and the
 fastest one is applied.  Results are cached per (GPU name, workload class) in a JSON file
 ($MB_AUTOTUNE_CACHE, default ~/.cache/mertens_k2/autotune.json); a workload class buckets the
@@ -20,6 +22,7 @@ import threading
 from . import k2
 
 SPACE = [(cpt, shift, scale) for cpt in (2, 3, 4) for shift in (0, 1) for scale in (0.5, 1.0, 2.0)]
+SCHEDULES = (0, 1)
 _lock = threading.Lock()
 
 
@@ -70,35 +73,45 @@ def _store(d: dict) -> None:
         pass                                    # a read-only home just disables the cache
 
 
-def autotune(plan: k2.Plan, reps: int = 3, use_cache: bool = True, space=SPACE) -> dict:
-    """Pick and apply the fastest configuration; returns {config, ms, timings, cached}."""
+def _apply(plan: k2.Plan, cfg) -> None:
+    plan.set_schedule(cfg[3] if len(cfg) > 3 else 0)
+    plan.configure(*cfg[:3])
+
+
+def autotune(plan: k2.Plan, reps: int = 3, use_cache: bool = True, space=SPACE, schedules=SCHEDULES) -> dict:
+    """Pick and apply the fastest configuration (light_cpt, nzw_shift, chunk_scale, schedule);
+    returns {config, ms, timings, cached}."""
     key = workload_key(plan)
     if use_cache:
         with _lock:
             hit = _load().get(key)
-        if hit:
-            plan.configure(*hit["config"])
+        if hit and len(hit["config"]) == 4:
+            _apply(plan, hit["config"])
             return {"config": tuple(hit["config"]), "ms": hit["ms"], "timings": hit.get("timings", {}),
                     "cached": True, "key": key}
     timings = {}
     best = None
-    if space == SPACE:                          # the library's own search over the same space
-        import ctypes as C
-        from ._lib import check, lib
-        cpt, shift, scale, ms = C.c_int(), C.c_int(), C.c_double(), C.c_double()
-        t = (C.c_double * len(SPACE))()
-        check(lib().mb_plan_autotune(plan.handle, int(reps), C.byref(cpt), C.byref(shift), C.byref(scale),
-                                     C.byref(ms), t))
-        timings = {f"{c}/{sh}/{sc}": t[i] for i, (c, sh, sc) in enumerate(SPACE)}
-        best = ((cpt.value, shift.value, scale.value), ms.value)
-    else:
-        for cfg in space:
-            plan.configure(*cfg)
-            ms = plan.time(reps)
-            timings[f"{cfg[0]}/{cfg[1]}/{cfg[2]}"] = ms
-            if best is None or ms < best[1]:
-                best = (cfg, ms)
-    plan.configure(*best[0])
+    for sched in schedules:
+        plan.set_schedule(sched)
+        if space == SPACE:                      # the library's own search over the same space
+            import ctypes as C
+            from ._lib import check, lib
+            cpt, shift, scale, ms = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+            t = (C.c_double * len(SPACE))()
+            check(lib().mb_plan_autotune(plan.handle, int(reps), C.byref(cpt), C.byref(shift), C.byref(scale),
+                                         C.byref(ms), t))
+            timings.update({f"{c}/{sh}/{sc}/{sched}": t[i] for i, (c, sh, sc) in enumerate(SPACE)})
+            cand = ((cpt.value, shift.value, scale.value, sched), ms.value)
+            if best is None or cand[1] < best[1]:
+                best = cand
+        else:
+            for cfg in space:
+                plan.configure(*cfg)
+                ms = plan.time(reps)
+                timings[f"{cfg[0]}/{cfg[1]}/{cfg[2]}/{sched}"] = ms
+                if best is None or ms < best[1]:
+                    best = ((*cfg, sched), ms)
+    _apply(plan, best[0])
     if use_cache:
         with _lock:
             d = _load()

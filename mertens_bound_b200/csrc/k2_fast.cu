@@ -341,6 +341,36 @@ k2_light_kernel(TabView t, CandView c, const FastItem *items, const FastGroup *g
     light_item<CPT, FUSED>(it, groups[it.group], t, c, partial, smem);
 }
 
+// Both tiers in one persistent kernel: two CTAs per SM pull items from one counter, the heavy
+// items first (largest first), then the light items (largest first), so the SMs stay busy to the
+// end without a second launch.  The light part runs at the heavy part's register budget
+// (launch bounds 256 x 2: at most 128 registers per thread).
+template <int CPT, bool FUSED>
+__global__ void __launch_bounds__(FAST_THREADS, 2)
+k2_tiers_kernel(TabView t, CandView c, const FastItem *items, int n_items, const FastGroup *groups, int *counter,
+                double *partial) {
+    __shared__ __align__(16) unsigned char smem[FAST_SMEM];
+    __shared__ double2 s_tab[HEAVY_TAB];
+    __shared__ int s_item;
+    for (int i = threadIdx.x; i < HEAVY_TAB; i += FAST_THREADS) {
+        double sn, cs;
+        sincospi((double)i * (2.0 / HEAVY_TAB), &sn, &cs);
+        s_tab[i] = make_double2(cs, sn);
+    }
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int idx = s_item;
+        if (idx >= n_items) break;
+        const FastItem it = items[idx];
+        if (it.tier == 0)
+            heavy_item<HEAVY_CPT>(it, groups[it.group], t, c, partial, smem, s_tab);
+        else
+            light_item<CPT, FUSED>(it, groups[it.group], t, c, partial, smem);
+    }
+}
+
 // One warp per candidate: lane l sums chunks l, l+32, ... of the candidate's group, then a fixed
 // shuffle tree adds the lanes (deterministic: the order depends only on the chunk count).
 __global__ void fast_reduce_kernel(const FastGroup *groups, int n_groups, const double *partial,
@@ -393,13 +423,44 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
     return MB_OK;
 }
 
+static int launch_tiers_one(const TabView &tv, const FastPlanDev &pd, CandView c, cudaStream_t s) {
+    const unsigned grid = pd.heavy_grid;
+    const int n = pd.n_heavy + pd.n_light;
+    if (pd.fused_phase) {
+        switch (pd.light_cpt) {
+            case 2: k2_tiers_kernel<2, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 3: k2_tiers_kernel<3, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            default: k2_tiers_kernel<4, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+        }
+    } else {
+        switch (pd.light_cpt) {
+            case 2: k2_tiers_kernel<2, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 3: k2_tiers_kernel<3, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            default: k2_tiers_kernel<4, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+        }
+    }
+    MB_CUDA(cudaGetLastError());
+    return MB_OK;
+}
+
 // tiers: bit 0 runs the heavy tier, bit 1 the light tier (3 = the full evaluation; a single
-// tier is used to time one kernel on its own -- the result then lacks the other tier).
+// tier is used to time one kernel on its own -- the result then lacks the other tier).  With
+// pd.one_kernel and both tiers, k2_tiers_kernel runs every item (its events are the light pair).
 int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
                 double *d_dk, cudaStream_t s, int tiers, const TierEvents *ev) {
     const TabView tv = view(t);
     const bool heavy = (tiers & 1) && pd.n_heavy > 0;
     const bool light = (tiers & 2) && pd.n_light > 0;
+    if (pd.one_kernel && heavy && light) {
+        MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), s));
+        if (ev) MB_CUDA(cudaEventRecord(ev->light0, s));
+        MB_TRY(launch_tiers_one(tv, pd, c, s));
+        if (ev) MB_CUDA(cudaEventRecord(ev->light1, s));
+        fast_reduce_kernel<<<(unsigned)((c.P * 32 + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
+                                                                         d_val, d_dd, d_dk);
+        MB_CUDA(cudaGetLastError());
+        return MB_OK;
+    }
     // with both tiers: fork the heavy tier onto the table's side stream, concurrently with the
     // light tier on s; with one tier everything stays on s
     const bool fork = heavy && light;

@@ -41,6 +41,8 @@ struct FastPlanDev {
     int light_cpt = 4;          // candidates per thread of the light kernel: 2, 3 or 4
     bool fused_phase = false;   // light tier on light_phase32_fused: every zero has gamma below
                                 // FUSED_PHASE_GAMMA, so G's integer part is below 2^19
+    bool one_kernel = false;    // both tiers in k2_tiers_kernel (one persistent kernel) instead of
+                                // the heavy kernel on a side stream beside the light kernel
     unsigned heavy_grid = 0;
     int *counter = nullptr;
     double *partial = nullptr;

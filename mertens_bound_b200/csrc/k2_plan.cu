@@ -28,6 +28,7 @@ struct mb_plan {
     std::vector<int> shape_nzw;
     std::vector<int64_t> heavy_chunk, light_chunk;
     int light_cpt = 4;
+    int schedule = 0;              // 0: two concurrent tier kernels, 1: one persistent kernel
     int nzw_shift = 0;             // extra doublings of the default warps-per-candidate-set split
     double chunk_scale = 1.0;      // multiplies the automatic work-item sizes
     int64_t z_begin = 0, z_end = INT64_MAX;   // zero-range shard of every group (default: all)
@@ -254,6 +255,7 @@ int upload(mb_plan *p) {
     p->dev.n_light = (int)p->items.size() - p->n_heavy_items;
     p->dev.n_groups = (int)p->groups.size();
     p->dev.light_cpt = p->light_cpt;
+    p->dev.one_kernel = p->schedule == 1;
     p->dev.fused_phase = p->table->h_gamma.empty() || p->table->h_gamma.back() < FUSED_PHASE_GAMMA;
     unsigned hg = 148;
     MB_TRY(heavy_grid_size(p->table->device, &hg));
@@ -424,6 +426,22 @@ extern "C" int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, doubl
     }
     MB_TRY(device_guard(p->table->device));
     return upload(p);
+}
+
+extern "C" int mb_plan_set_schedule(mb_plan *p, int schedule) {
+    MB_CHECK_ARG(p, "mb_plan_set_schedule: null plan");
+    MB_CHECK_ARG(schedule == 0 || schedule == 1, "mb_plan_set_schedule: schedule=%d (0 or 1)", schedule);
+    MB_TRY(device_guard(p->table->device));
+    p->schedule = schedule;
+    p->dev.one_kernel = schedule == 1;
+    free_io(p);                    // the captured graph holds the old launch sequence
+    return MB_OK;
+}
+
+extern "C" int mb_plan_schedule(const mb_plan *p, int *schedule) {
+    MB_CHECK_ARG(p && schedule, "mb_plan_schedule: null argument");
+    *schedule = p->schedule;
+    return MB_OK;
 }
 
 // Give the share skip_frac (0 .. 1/4) of tol to not evaluating each group's negligible tail: the

@@ -178,6 +178,16 @@ class Plan:
         check(_lib.lib().mb_plan_configure(self.handle, int(light_cpt), int(nzw_shift), float(chunk_scale)))
         self.config = (int(light_cpt), int(nzw_shift), float(chunk_scale))
 
+    def set_schedule(self, schedule: int):
+        """0: the two tier kernels run concurrently (heavy persistent kernel on a side stream);
+        1: one persistent kernel runs both tiers' items."""
+        check(_lib.lib().mb_plan_set_schedule(self.handle, int(schedule)))
+
+    def schedule(self) -> int:
+        s = C.c_int()
+        check(_lib.lib().mb_plan_schedule(self.handle, C.byref(s)))
+        return s.value
+
     def time(self, reps: int = 3) -> float:
         """Median device milliseconds of one run (synthetic candidates)."""
         ms = C.c_double()
