@@ -948,7 +948,8 @@ def run_profile_case(args):
               thread) args.warmup + args.steps times, then the plain kernel once (~40 MB on the
               device);
       search  the bench workload (zeros below 3e5, 4,096 candidates): the plain kernel once, the
-              light tier alone at 2, 3 and 4 candidates per thread, the heavy tier alone (~80 MB)."""
+              light tier alone at 2, 3 and 4 candidates per thread, the heavy tier alone, then both
+              tiers in one persistent kernel at 4 candidates per thread (~80 MB)."""
     if args.profile_case == "extras":
         return run_profile_extras()
     if args.profile_case == "scoring":
@@ -989,6 +990,8 @@ def run_profile_case(args):
             plan.configure(cpt, 0, 1.0)
             tiers(2)
         tiers(1)
+        plan.set_schedule(1)          # both tiers in one persistent kernel (k2_tiers_kernel)
+        tiers(3)
     torch.cuda.synchronize(dev)
     ht, lt = C_double_pair(L.mb_plan_tier_terms, plan.handle)
     print(json.dumps({"profile_case": args.profile_case, "zeros": table.count_below(T), "candidates": P,
