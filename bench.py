@@ -403,7 +403,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * P, "d2h_bytes_per_step": 3 * 8 * P},
         "roofline": roofline,
         "clocks": clocks,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": (2 if one_kernel else 3) * args.steps,
         "wall_s_timed_region": wall_s,
         "accuracy": {"err_vs_certified": {"candidates": 64, "max_abs_err": err_vs_cert,
                                           "max_interval_width": float(np.max(chi - clo)),

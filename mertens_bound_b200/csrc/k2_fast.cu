@@ -128,19 +128,36 @@ MB_DEV void light_tile(const void *tile_v, int nt, int zl, int ZL, const CandReg
     flush();
 }
 
-// sin/cos(2 pi y) for any y (turns): y = q/1024 + r with |r| <= 2^-11 (exact), the table
-// entry (cos, sin)(2 pi q/1024) rotated by r through short polynomials (truncation below 3e-15).
-constexpr int HEAVY_TAB = 1024;
+// sin/cos(2 pi y) for any y (turns): y = q/2048 + r with |r| <= 2^-12 (exact), the table
+// entry (cos, sin)(2 pi q/2048) rotated by r: sin(2 pi r) = r (2pi - (2pi)^3 r^2 / 6) (truncation
+// 7e-17) and cos(2 pi r) - 1 = C r^2 with C the minimax constant on |r| <= 2^-12 (-(2pi)^2/2 +
+// 3.2e-6: error 3.96e-14, computed with mpmath), so the cosine costs one product.
+constexpr int HEAVY_TAB = 2048;
+constexpr int HEAVY_TAB_BYTES = HEAVY_TAB * (int)sizeof(double2);
 MB_DEV void sincos_turns_tab(double y, const double2 *tab, double &sn, double &cs) {
     const double m = fma(y, (double)HEAVY_TAB, MB_MAGIC);
     const int q = __double2loint(m) & (HEAVY_TAB - 1);
     const double r = fma(-1.0 / HEAVY_TAB, m - MB_MAGIC, y);
     const double u = r * r;
     const double s = r * fma(u, -41.341702240399755, 6.283185307179586);     // sin(2 pi r)
-    const double cm1 = u * fma(u, 64.93939402266828, -19.739208802178716);  // cos(2 pi r) - 1
+    const double cm1 = u * -19.739205595594533;                            // cos(2 pi r) - 1
     const double2 T = tab[q];
     cs = fma(T.x, cm1, fma(-T.y, s, T.x));
     sn = fma(T.y, cm1, fma(T.x, s, T.y));
+}
+
+// The heavy tier's shared memory: the staged tile / reduction buffer, then the (cos, sin) table
+// (dynamic shared memory: 24 KB + 32 KB is above the 48 KB static limit).
+constexpr int HEAVY_DSMEM = FAST_SMEM + HEAVY_TAB_BYTES;
+
+MB_DEV double2 *heavy_table_init(unsigned char *dsm) {
+    double2 *tab = reinterpret_cast<double2 *>(dsm + FAST_SMEM);
+    for (int i = threadIdx.x; i < HEAVY_TAB; i += FAST_THREADS) {
+        double sn, cs;
+        sincospi((double)i * (2.0 / HEAVY_TAB), &sn, &cs);
+        tab[i] = make_double2(cs, sn);
+    }
+    return tab;
 }
 
 template <int CPT>
@@ -313,14 +330,9 @@ MB_DEV void heavy_item(const FastItem &it, const FastGroup &gr, const TabView &t
 __global__ void __launch_bounds__(FAST_THREADS, 2)
 k2_heavy_kernel(TabView t, CandView c, const FastItem *items, int n_items, const FastGroup *groups,
                 int *counter, double *partial) {
-    __shared__ __align__(16) unsigned char smem[FAST_SMEM];
-    __shared__ double2 s_tab[HEAVY_TAB];
+    extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
-    for (int i = threadIdx.x; i < HEAVY_TAB; i += FAST_THREADS) {
-        double sn, cs;
-        sincospi((double)i * (2.0 / HEAVY_TAB), &sn, &cs);
-        s_tab[i] = make_double2(cs, sn);
-    }
+    const double2 *s_tab = heavy_table_init(smem);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -349,14 +361,9 @@ template <int CPT, bool FUSED>
 __global__ void __launch_bounds__(FAST_THREADS, 2)
 k2_tiers_kernel(TabView t, CandView c, const FastItem *items, int n_items, const FastGroup *groups, int *counter,
                 double *partial) {
-    __shared__ __align__(16) unsigned char smem[FAST_SMEM];
-    __shared__ double2 s_tab[HEAVY_TAB];
+    extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
-    for (int i = threadIdx.x; i < HEAVY_TAB; i += FAST_THREADS) {
-        double sn, cs;
-        sincospi((double)i * (2.0 / HEAVY_TAB), &sn, &cs);
-        s_tab[i] = make_double2(cs, sn);
-    }
+    const double2 *s_tab = heavy_table_init(smem);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -423,20 +430,40 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
     return MB_OK;
 }
 
+// Opt every kernel that holds the heavy table into HEAVY_DSMEM bytes of dynamic shared memory (once
+// per device; the attribute is per device and function).
+static int heavy_smem_attributes() {
+    static bool done[64] = {};
+    int dev = 0;
+    MB_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev]) return MB_OK;
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    MB_CUDA(cudaFuncSetAttribute(k2_heavy_kernel, a, HEAVY_DSMEM));
+    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<2, true>, a, HEAVY_DSMEM));
+    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<3, true>, a, HEAVY_DSMEM));
+    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<4, true>, a, HEAVY_DSMEM));
+    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<2, false>, a, HEAVY_DSMEM));
+    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<3, false>, a, HEAVY_DSMEM));
+    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<4, false>, a, HEAVY_DSMEM));
+    if (dev >= 0 && dev < 64) done[dev] = true;
+    return MB_OK;
+}
+
 static int launch_tiers_one(const TabView &tv, const FastPlanDev &pd, CandView c, cudaStream_t s) {
     const unsigned grid = pd.heavy_grid;
     const int n = pd.n_heavy + pd.n_light;
+    const size_t sm = HEAVY_DSMEM;
     if (pd.fused_phase) {
         switch (pd.light_cpt) {
-            case 2: k2_tiers_kernel<2, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            case 3: k2_tiers_kernel<3, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            default: k2_tiers_kernel<4, true><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 2: k2_tiers_kernel<2, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 3: k2_tiers_kernel<3, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            default: k2_tiers_kernel<4, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
         }
     } else {
         switch (pd.light_cpt) {
-            case 2: k2_tiers_kernel<2, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            case 3: k2_tiers_kernel<3, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            default: k2_tiers_kernel<4, false><<<grid, FAST_THREADS, 0, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 2: k2_tiers_kernel<2, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 3: k2_tiers_kernel<3, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            default: k2_tiers_kernel<4, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
         }
     }
     MB_CUDA(cudaGetLastError());
@@ -451,6 +478,7 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
     const TabView tv = view(t);
     const bool heavy = (tiers & 1) && pd.n_heavy > 0;
     const bool light = (tiers & 2) && pd.n_light > 0;
+    if (heavy) MB_TRY(heavy_smem_attributes());
     if (pd.one_kernel && heavy && light) {
         MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), s));
         if (ev) MB_CUDA(cudaEventRecord(ev->light0, s));
@@ -472,8 +500,8 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
         }
         MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), hs));
         if (ev) MB_CUDA(cudaEventRecord(ev->heavy0, hs));
-        k2_heavy_kernel<<<pd.heavy_grid, FAST_THREADS, 0, hs>>>(tv, c, pd.items, pd.n_heavy, pd.groups,
-                                                                pd.counter, pd.partial);
+        k2_heavy_kernel<<<pd.heavy_grid, FAST_THREADS, HEAVY_DSMEM, hs>>>(tv, c, pd.items, pd.n_heavy, pd.groups,
+                                                                          pd.counter, pd.partial);
         MB_CUDA(cudaGetLastError());
         if (ev) MB_CUDA(cudaEventRecord(ev->heavy1, hs));
         if (fork) MB_CUDA(cudaEventRecord(t.ev_join, t.side));

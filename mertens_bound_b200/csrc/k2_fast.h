@@ -56,8 +56,9 @@ struct FastPlanDev {
 //          + phase 4.5 2^-32 turn (2.4 with light_phase32_fused; 7e-9 rad) + amplitude and FFMA
 //          roundings (2 2^-24) + FP32 summation over a 16-term flush window (15 2^-24)
 //          ->  2.03e-6, held at 2.2e-6
-//   heavy: phase 2^-47 turn, table + polynomial 3e-15, FP64 roundings  ->  2e-13 (kept loose:
-//          the heavy amplitude sum is O(1), so this share of the bound is negligible)
+//   heavy: phase 2^-47 turn (4.5e-14 rad), 2048-entry table + polynomials (cos 3.96e-14, sin
+//          7e-17), FP64 roundings  ->  ~9e-14, held at 2e-13 (loose: the heavy amplitude sum is
+//          O(1), so this share of the bound is negligible)
 constexpr double EPS_LIGHT = 2.2e-6;
 // 2 pi (2^19 - 1): below it G = gamma / 2pi has an integer part below 2^19
 constexpr double FUSED_PHASE_GAMMA = 6.283185307179586 * 524287.0;
