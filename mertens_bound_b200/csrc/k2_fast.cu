@@ -431,8 +431,9 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
 }
 
 // Opt every kernel that holds the heavy table into HEAVY_DSMEM bytes of dynamic shared memory (once
-// per device; the attribute is per device and function).
-static int heavy_smem_attributes() {
+// per device; the attribute is per device and function).  Plans call it when they are built, so
+// a first launch inside a stream capture finds it done.
+int heavy_smem_attributes() {
     static bool done[64] = {};
     int dev = 0;
     MB_CUDA(cudaGetDevice(&dev));

@@ -41,8 +41,9 @@ struct FastPlanDev {
     int light_cpt = 4;          // candidates per thread of the light kernel: 2, 3 or 4
     bool fused_phase = false;   // light tier on light_phase32_fused: every zero has gamma below
                                 // FUSED_PHASE_GAMMA, so G's integer part is below 2^19
-    bool one_kernel = false;    // both tiers in k2_tiers_kernel (one persistent kernel) instead of
-                                // the heavy kernel on a side stream beside the light kernel
+    bool one_kernel = false;    // both tiers in k2_tiers_kernel (one persistent kernel, items in
+                                // plan order) instead of the heavy kernel on a side stream beside
+                                // the light kernel
     unsigned heavy_grid = 0;
     int *counter = nullptr;
     double *partial = nullptr;
@@ -74,6 +75,8 @@ struct TierEvents {
 int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val, double *d_dd,
                 double *d_dk, cudaStream_t s, int tiers = 3, const TierEvents *ev = nullptr);
 int heavy_grid_size(int device, unsigned *grid);
+// Dynamic shared memory opt-in of the kernels holding the heavy tier's table (current device).
+int heavy_smem_attributes();
 int calibrate_issue(int device, double *thread_inst_per_s);
 // Measured full-rate throughput of the three pipes the tier kernels use, in thread operations
 // per second: FFMA (FMA pipe), MUFU sin/cos (XU pipe), DFMA (FP64 pipe).

@@ -232,8 +232,31 @@ int build_items(mb_plan *p, int sms) {
     std::stable_sort(heavy.begin(), heavy.end(), by_cost);
     std::stable_sort(light.begin(), light.end(), by_cost);
     p->n_heavy_items = (int)heavy.size();
-    p->items = heavy;
-    p->items.insert(p->items.end(), light.begin(), light.end());
+    if (p->schedule == 2) {
+        // one kernel, tiers interleaved in proportion to their estimated cost (a heavy term costs
+        // ~3.5 light terms), so the two CTAs of an SM mostly hold one item of each tier: the FP64-
+        // bound heavy work and the XU-bound light work share the SM's issue slots
+        auto cost = [](const FastItem &a) { return (a.tier == 0 ? 3.5 : 1.0) * a.nc * (double)(a.z1 - a.z0); };
+        double th = 0, tl = 0, dh = 0, dl = 0;
+        for (const FastItem &a : heavy) th += cost(a);
+        for (const FastItem &a : light) tl += cost(a);
+        p->items.clear();
+        size_t ih = 0, il = 0;
+        while (ih < heavy.size() || il < light.size()) {
+            const bool take_h = il >= light.size() ||
+                                (ih < heavy.size() && dh / std::max(th, 1.0) <= dl / std::max(tl, 1.0));
+            if (take_h) {
+                dh += cost(heavy[ih]);
+                p->items.push_back(heavy[ih++]);
+            } else {
+                dl += cost(light[il]);
+                p->items.push_back(light[il++]);
+            }
+        }
+    } else {
+        p->items = heavy;
+        p->items.insert(p->items.end(), light.begin(), light.end());
+    }
     p->partial_doubles = (size_t)std::max<int64_t>(pbase, 3);
     return MB_OK;
 }
@@ -241,6 +264,8 @@ int build_items(mb_plan *p, int sms) {
 int upload(mb_plan *p) {
     free_dev(p);
     free_io(p);
+    MB_TRY(device_guard(p->table->device));
+    MB_TRY(heavy_smem_attributes());
     int sms = 148;
     MB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->table->device));
     MB_TRY(build_items(p, sms));
@@ -255,7 +280,7 @@ int upload(mb_plan *p) {
     p->dev.n_light = (int)p->items.size() - p->n_heavy_items;
     p->dev.n_groups = (int)p->groups.size();
     p->dev.light_cpt = p->light_cpt;
-    p->dev.one_kernel = p->schedule == 1;
+    p->dev.one_kernel = p->schedule >= 1;
     p->dev.fused_phase = p->table->h_gamma.empty() || p->table->h_gamma.back() < FUSED_PHASE_GAMMA;
     unsigned hg = 148;
     MB_TRY(heavy_grid_size(p->table->device, &hg));
@@ -430,10 +455,12 @@ extern "C" int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, doubl
 
 extern "C" int mb_plan_set_schedule(mb_plan *p, int schedule) {
     MB_CHECK_ARG(p, "mb_plan_set_schedule: null plan");
-    MB_CHECK_ARG(schedule == 0 || schedule == 1, "mb_plan_set_schedule: schedule=%d (0 or 1)", schedule);
+    MB_CHECK_ARG(schedule >= 0 && schedule <= 2, "mb_plan_set_schedule: schedule=%d (0, 1 or 2)", schedule);
     MB_TRY(device_guard(p->table->device));
+    const bool reorder = (schedule == 2) != (p->schedule == 2);
     p->schedule = schedule;
-    p->dev.one_kernel = schedule == 1;
+    if (reorder) return upload(p);     // the item order changes
+    p->dev.one_kernel = schedule >= 1;
     free_io(p);                    // the captured graph holds the old launch sequence
     return MB_OK;
 }

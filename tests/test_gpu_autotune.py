@@ -16,8 +16,8 @@ def test_autotune_picks_and_caches(gpu, small_table, tmp_path, monkeypatch):
     with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [1000, 500], [3e-9, 1e-9], [math.inf, 20000.0]) as plan:
         ref, _, _ = plan.run(cd)
         r = autotune.autotune(plan, reps=2)
-        assert not r["cached"] and tuple(r["config"][:3]) in autotune.SPACE and r["config"][3] in (0, 1)
-        assert len(r["timings"]) == 2 * len(autotune.SPACE) and min(r["timings"].values()) == r["ms"]
+        assert not r["cached"] and tuple(r["config"][:3]) in autotune.SPACE and r["config"][3] in (0, 1, 2)
+        assert len(r["timings"]) == 3 * len(autotune.SPACE) and min(r["timings"].values()) == r["ms"]
         assert plan.schedule() == r["config"][3]
         val, _, _ = plan.run(cd)
         eb = max(plan.group_info(g)["err_bound"] for g in range(2))
@@ -28,8 +28,8 @@ def test_autotune_picks_and_caches(gpu, small_table, tmp_path, monkeypatch):
 
 @pytest.mark.parametrize("cpt", [2, 3, 4])
 def test_schedules_give_the_same_bits(gpu, small_table, cpt):
-    """One persistent kernel for both tiers runs the same items with the same per-item arithmetic
-    as the two concurrent kernels, so every output bit agrees."""
+    """One persistent kernel for both tiers (in plan order or interleaved) runs the same items with
+    the same per-item arithmetic as the two concurrent kernels, so every output bit agrees."""
     cd = synth.make_candidates(700, seed=32)
     cd.delta[:] = np.random.default_rng(33).uniform(-1e-4, 1e-4, cd.n)
     with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [300, 400], [3e-9, 1.5e-10], [math.inf, 20000.0],
@@ -41,7 +41,9 @@ def test_schedules_give_the_same_bits(gpu, small_table, cpt):
         plan.set_schedule(1)
         assert plan.schedule() == 1
         b = plan.run(cd)
+        plan.set_schedule(2)
+        d = plan.run(cd)
         plan.set_schedule(0)
         c = plan.run(cd)
-    for x, y, z in zip(a, b, c):
-        assert np.array_equal(x, y) and np.array_equal(x, z)
+    for x, y, z, w in zip(a, b, c, d):
+        assert np.array_equal(x, y) and np.array_equal(x, z) and np.array_equal(x, w)
