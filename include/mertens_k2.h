@@ -216,7 +216,8 @@ int mb_plan_run_dev(mb_plan *p, const uint64_t *d_v_int, const uint64_t *d_v_fra
 int mb_plan_run(mb_plan *p, const uint64_t *v_int, const uint64_t *v_frac, const double *delta,
                 double *val, double *dd, double *dk);
 /* Run one tier only (tiers: 1 heavy, 2 light, 3 both = mb_plan_run_dev), to time a kernel on
- * its own; with 1 or 2 the results miss the other tier's terms.  No reference counterpart. */
+ * its own; with 1 or 2 the results hold that tier's terms only (the other tier's partial sums are
+ * cleared first).  No reference counterpart. */
 int mb_plan_run_tiers_dev(mb_plan *p, int tiers, const uint64_t *d_v_int, const uint64_t *d_v_frac,
                           const double *d_delta, double *d_val, double *d_dd, double *d_dk, void *stream);
 /* Zero-terms per run in each tier. */

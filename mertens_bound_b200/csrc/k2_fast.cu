@@ -494,6 +494,8 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
     // light tier on s; with one tier everything stays on s
     const bool fork = heavy && light;
     cudaStream_t hs = fork ? t.side : s;
+    // a one-tier run: the other tier's partial sums count as zero, not as a previous run's values
+    if ((tiers & 3) != 3) MB_CUDA(cudaMemsetAsync(pd.partial, 0, pd.partial_bytes, s));
     if (heavy) {
         if (fork) {
             MB_CUDA(cudaEventRecord(t.ev_fork, s));

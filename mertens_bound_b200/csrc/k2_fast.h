@@ -47,6 +47,7 @@ struct FastPlanDev {
     unsigned heavy_grid = 0;
     int *counter = nullptr;
     double *partial = nullptr;
+    size_t partial_bytes = 0;   // size of `partial` (a one-tier run clears it first)
 };
 
 // Per-term worst-case absolute error of cos/sin (times amplitude) in each tier, per unit of

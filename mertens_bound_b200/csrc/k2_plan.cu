@@ -273,6 +273,7 @@ int upload(mb_plan *p) {
     MB_CUDA(cudaMalloc(&p->dev.groups, std::max<size_t>(1, p->groups.size()) * sizeof(FastGroup)));
     MB_CUDA(cudaMalloc(&p->dev.counter, sizeof(int)));
     MB_CUDA(cudaMalloc(&p->dev.partial, p->partial_doubles * sizeof(double)));
+    p->dev.partial_bytes = p->partial_doubles * sizeof(double);
     if (!p->items.empty())
         MB_CUDA(cudaMemcpy(p->dev.items, p->items.data(), p->items.size() * sizeof(FastItem), cudaMemcpyHostToDevice));
     MB_CUDA(cudaMemcpy(p->dev.groups, p->groups.data(), p->groups.size() * sizeof(FastGroup), cudaMemcpyHostToDevice));
