@@ -27,17 +27,32 @@ struct Cand64 {
 MB_DEV Cand64 fold_delta(uint64_t vi, uint64_t vf, double delta) {
     Cand64 c{vi, vf};
     if (delta != 0.0) {
-        double fl = floor(delta);
-        double fr = delta - fl;                         // exact for |delta| < 2^52, in [0,1)
-        double sc = fr * 18446744073709551616.0;        // fr 2^64, exact scaling
-        uint64_t add;
-        int64_t carry_int = (int64_t)fl;
-        if (sc >= 18446744073709551616.0) { add = 0; carry_int += 1; }
-        else add = (uint64_t)__double2ull_rn(sc);
-        uint64_t nf = vf + add;
-        carry_int += (nf < vf) ? 1 : 0;
-        c.vf = nf;
-        c.vi = vi + (uint64_t)carry_int;
+        // delta = M 2^(e - 53) exactly (|M| < 2^53), so delta 2^64 = M 2^sh: its 128-bit magnitude,
+        // rounded to the nearest integer (half up) when sh < 0, is added to or subtracted from v.
+        // Every step is exact (1 + delta, say, would round for small negative delta).
+        int e;
+        const double m = frexp(delta, &e);
+        const uint64_t am = (uint64_t)fabs(ldexp(m, 53));
+        const int sh = e + 11;                          // e - 53 + 64
+        uint64_t hi = 0, lo = 0;
+        if (sh >= 64) {
+            hi = am << (sh - 64);
+        } else if (sh > 0) {
+            hi = am >> (64 - sh);
+            lo = am << sh;
+        } else if (sh == 0) {
+            lo = am;
+        } else if (sh > -64) {
+            lo = (am + (1ull << (-sh - 1))) >> (-sh);
+        }
+        if (delta > 0.0) {
+            const uint64_t nf = vf + lo;
+            c.vf = nf;
+            c.vi = vi + hi + (nf < vf ? 1u : 0u);
+        } else {
+            c.vf = vf - lo;
+            c.vi = vi - hi - (vf < lo ? 1u : 0u);
+        }
     }
     return c;
 }
