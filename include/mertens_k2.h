@@ -235,8 +235,9 @@ int mb_calibrate_pipes(int device, double *ffma_per_s, double *mufu_per_s, doubl
  * host-pointer runs (its CUDA graph) record nothing.  No reference counterpart. */
 int mb_plan_kernel_timing(mb_plan *p, int n_slots);
 /* The light and heavy kernel times (ms) of the last min(n, n_slots, runs) timed runs, oldest
- * first, in light_ms / heavy_ms (-1 where that tier did not run); *n_out = how many.  Waits for
- * those runs' events. */
+ * first, in light_ms / heavy_ms (-1 where that tier did not run); *n_out = how many.  Under a
+ * one-kernel schedule (mb_plan_set_schedule 1 or 2) a run of both tiers is one launch: its time
+ * is in light_ms and heavy_ms is -1.  Waits for those runs' events. */
 int mb_plan_kernel_times(mb_plan *p, int n, double *light_ms, double *heavy_ms, int *n_out);
 
 /* Batched Newton polish of the offsets: h0 = K2 at the given d_delta; then up to `iters` steps

@@ -302,8 +302,9 @@ int plan_run_timed(mb_plan *p, int tiers, const uint64_t *vi, const uint64_t *vf
     if (!p->tev.empty()) {
         const size_t slot = (size_t)(p->tev_runs % (long long)p->tev.size());
         ev = &p->tev[slot];
-        p->tev_tiers[slot] = (signed char)(((tiers & 1) && p->dev.n_heavy > 0 ? 1 : 0) |
-                                           ((tiers & 2) && p->dev.n_light > 0 ? 2 : 0));
+        int ran = ((tiers & 1) && p->dev.n_heavy > 0 ? 1 : 0) | ((tiers & 2) && p->dev.n_light > 0 ? 2 : 0);
+        if (ran == 3 && p->dev.one_kernel) ran = 2;      // one kernel: its time is the light pair
+        p->tev_tiers[slot] = (signed char)ran;
         ++p->tev_runs;
     }
     return launch_fast(*p->table, p->dev, CandView{vi, vf, delta, p->P}, val, dd, dk, s, tiers, ev);

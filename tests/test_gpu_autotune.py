@@ -47,3 +47,37 @@ def test_schedules_give_the_same_bits(gpu, small_table, cpt):
         c = plan.run(cd)
     for x, y, z, w in zip(a, b, c, d):
         assert np.array_equal(x, y) and np.array_equal(x, z) and np.array_equal(x, w)
+
+
+def test_kernel_timing_hook(gpu, small_table):
+    """mb_plan_kernel_timing / mb_plan_kernel_times: per-run tier kernel durations under each
+    schedule (one launch under the one-kernel schedules, reported as the light time)."""
+    import ctypes as C
+
+    import torch
+    from mertens_bound_b200._lib import check, lib
+    L = lib()
+    dev = torch.device("cuda", 0)
+    cd = synth.make_candidates(512, seed=34)
+    vi = torch.from_numpy(cd.v_int.view(np.int64).copy()).to(dev)
+    vf = torch.from_numpy(cd.v_frac.view(np.int64).copy()).to(dev)
+    out = torch.empty(3, 512, dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [512], [3e-9], [math.inf], tol=1e-8) as plan:
+        for sched in (0, 1, 2):
+            plan.set_schedule(sched)
+            check(L.mb_plan_kernel_timing(plan.handle, 4))
+            for tiers in (3, 3, 1, 2):
+                check(L.mb_plan_run_tiers_dev(plan.handle, tiers, vi.data_ptr(), vf.data_ptr(), None,
+                                              out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), s))
+            lt, ht, n = (C.c_double * 4)(), (C.c_double * 4)(), C.c_int()
+            check(L.mb_plan_kernel_times(plan.handle, 4, lt, ht, C.byref(n)))
+            assert n.value == 4
+            both_heavy = [ht[0], ht[1]]
+            assert all(x > 0 for x in (lt[0], lt[1], ht[2], lt[3]))
+            assert ht[3] == -1 and lt[2] == -1
+            if sched == 0:
+                assert all(x > 0 for x in both_heavy)
+            else:
+                assert all(x == -1 for x in both_heavy)
+            check(L.mb_plan_kernel_timing(plan.handle, 0))
