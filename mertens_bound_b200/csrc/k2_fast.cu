@@ -36,13 +36,12 @@ namespace mb {
 
 struct __align__(16) ZLight {   // 64 B
     uint32_t b0, b1, gi, psi32;  // psi32 = round(psi 2^32) + 2 (centres the truncation bias)
-                                 //         + LIGHT_ANG_BIAS (the angle's quantisation, light_angle)
     double b0s, c1s, gis, b1s;   // limb 2^-32 (exact)
     float a, b, d, pad;          // a = 2|c|w, b = -a gamma, d = -a gamma^2
 };
 
 struct __align__(16) ZLightF {  // 48 B: the light record of light_phase32_fused
-    uint32_t b0, b1, psi32;      // as in ZLight, psi32 = round(psi 2^32) + 1 + LIGHT_ANG_BIAS
+    uint32_t b0, b1, psi32;      // as in ZLight, psi32 = round(psi 2^32) + 1
     float a;                     // a = 2|c|w
     double b0s, c1s;             // limb 2^-32 (exact)
     double gh;                   // gI 2^32 + b1 (exact for gI < 2^19)
@@ -68,20 +67,13 @@ static_assert(sizeof(ZLightF) == 48, "fused light record");
 static_assert(FAST_SMEM >= HEAVY_TILE * sizeof(ZHeavy), "heavy tile");
 static_assert(FAST_SMEM >= FAST_THREADS * 4 * 3 * sizeof(double), "reduction buffer");
 
-// The angle 2pi u 2^-32 of a light term in radians without an int->float conversion (those
-// share the XU pipe with MUFU sin/cos): k = u >> 9 (arithmetic shift, so u is quantised to 2^-23
-// turn) becomes the float 1.5 2^23 + k by writing 0x4B400000 + k as its bits, and one FFMA gives
-// th = fl((1.5 2^23 + k) C - M) with C = fl(2pi) 2^-23 and M = 1.5 2^23 C rounded down to a
-// float.  So th = fl(C (k + 0.31831)): the offset 1.5 2^23 C - M = 2^-22 rad is 162.97 units of
-// 2^-32 turn, and the record's psi32 carries +93 (= 256 - 163) so that k + 0.31831 is u 2^-9
-// rounded to nearest (error <= 2^-24 turn + 0.03 units of 2^-32).  |th| <= 3.1415924 < pi for every
-// k in [-2^22, 2^22): inside the range where __sinf / __cosf have their documented error bounds.
-constexpr float LIGHT_ANG_C = 6.2831854820251465f * 1.1920928955078125e-07f;   // fl(2pi) 2^-23
-constexpr float LIGHT_ANG_M = 9.424777984619140625f;                          // 9882596 2^-20
-constexpr uint32_t LIGHT_ANG_BIAS = 93u;
-MB_DEV float light_angle(int32_t u) {
-    return fmaf(__int_as_float(0x4B400000 + (u >> 9)), LIGHT_ANG_C, -LIGHT_ANG_M);
-}
+// The angle 2pi u 2^-32 of a light term in radians: u (the signed phase in units of 2^-32 turn)
+// converted to float, times fl_down(2pi) 2^-32 -- rounded down so that |th| <= 2^31 C =
+// 3.14159250 < pi for every u, inside the range where __sinf / __cosf have their documented error
+// bounds.  (A conversion-free form -- the bits 0x4B400000 + (u >> 9) as a float and one FFMA --
+// measured 1-3% slower: the kernel is latency-bound, not XU-bound, and its chain is longer.)
+constexpr float LIGHT_ANG_C = 6.2831850051879883f * 2.3283064365386963e-10f;   // fl_down(2pi) 2^-32
+MB_DEV float light_angle(int32_t u) { return (float)u * LIGHT_ANG_C; }
 
 template <int CPT, bool FUSED>
 MB_DEV void light_tile(const void *tile_v, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
@@ -191,7 +183,7 @@ MB_DEV void stage_light(const TabView &t, int64_t j, double k, const double *w, 
     double a = 2.0 * t.alpha[j] * (w ? w[j] : exp(-k * g * g));
     uint32_t b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j], c1 = t.g1[j];
     r.b0 = b0; r.b1 = b1; r.gi = gi;
-    r.psi32 = (uint32_t)((t.psi[j] + 0x80000000ull) >> 32) + 2u + LIGHT_ANG_BIAS;
+    r.psi32 = (uint32_t)((t.psi[j] + 0x80000000ull) >> 32) + 2u;
     r.b0s = u32_to_f64(b0) * TWO_M32;
     r.c1s = u32_to_f64(c1) * TWO_M32;
     r.gis = u32_to_f64(gi) * TWO_M32;
@@ -208,8 +200,8 @@ MB_DEV void stage_light(const TabView &t, int64_t j, double k, const double *w, 
     uint32_t b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j], c1 = t.g1[j];
     r.b0 = b0; r.b1 = b1;
     // + 1 centres the fused phase's truncation (dropped products in [0, 3) units): error within
-    // +-2.4 units of 2^-32 turn; + LIGHT_ANG_BIAS centres the angle's quantisation
-    r.psi32 = (uint32_t)((t.psi[j] + 0x80000000ull) >> 32) + 1u + LIGHT_ANG_BIAS;
+    // +-2.4 units of 2^-32 turn
+    r.psi32 = (uint32_t)((t.psi[j] + 0x80000000ull) >> 32) + 1u;
     r.b0s = u32_to_f64(b0) * TWO_M32;
     r.c1s = u32_to_f64(c1) * TWO_M32;
     r.gh = fma(u32_to_f64(gi), 4294967296.0, u32_to_f64(b1));

@@ -52,12 +52,12 @@ struct FastPlanDev {
 
 // Per-term worst-case absolute error of cos/sin (times amplitude) in each tier, per unit of
 // amplitude a_j = 2|c_j| w_j:
-//   light: __sinf / __cosf on [-pi, pi] (documented 2^-21.41 / 2^-21.19, 4.2e-7, their internal
-//          argument scaling included) + the angle (light_angle: quantisation to 2^-23 turn,
-//          2^-24 turn = 3.75e-7 rad; FFMA rounding 2^-23 rad; fl(2pi) 3e-8 relative, 9e-8 rad)
+//   light: __sinf / __cosf on [-pi, pi] (documented 2^-21.41 / 2^-21.19, so 4.2e-7, their
+//          internal argument scaling included) + the angle (light_angle: int->float 2^-26 turn =
+//          9.4e-8 rad, the FMUL's rounding 2^-23 rad, fl_down(2pi) 4.8e-8 relative = 1.5e-7 rad)
 //          + phase 4.5 2^-32 turn (2.4 with light_phase32_fused; 7e-9 rad) + amplitude and FFMA
 //          roundings (2 2^-24) + FP32 summation over a 16-term flush window (15 2^-24)
-//          ->  2.03e-6, held at 2.2e-6
+//          ->  1.8e-6, held at 2.2e-6
 //   heavy: phase 2^-47 turn (4.5e-14 rad), 2048-entry table + polynomials (cos 3.96e-14, sin
 //          7e-17), FP64 roundings  ->  ~9e-14, held at 2e-13 (loose: the heavy amplitude sum is
 //          O(1), so this share of the bound is negligible)
