@@ -55,13 +55,13 @@ struct FastPlanDev {
 //   light: __sinf / __cosf on [-pi, pi] (documented 2^-21.41 / 2^-21.19, so 4.2e-7, their
 //          internal argument scaling included) + the angle (light_angle: int->float 2^-26 turn =
 //          9.4e-8 rad, the FMUL's rounding 2^-23 rad, fl_down(2pi) 4.8e-8 relative = 1.5e-7 rad)
-//          + phase 4.5 2^-32 turn (2.4 with light_phase32_fused; 7e-9 rad) + amplitude and FFMA
-//          roundings (2 2^-24) + FP32 summation over a 16-term flush window (15 2^-24)
-//          ->  1.8e-6, held at 2.2e-6
+//          + phase 4.5 2^-32 turn (2.4 with light_phase32_fused; 7e-9 rad): 7.9e-7 in cos / sin;
+//          + amplitude and FFMA roundings (2 2^-24) + FP32 summation over a 16-term flush window
+//          (15 2^-24): 1.01e-6  ->  1.80e-6, held at 1.9e-6
 //   heavy: phase 2^-47 turn (4.5e-14 rad), 2048-entry table + polynomials (cos 3.96e-14, sin
 //          7e-17), FP64 roundings  ->  ~9e-14, held at 2e-13 (loose: the heavy amplitude sum is
 //          O(1), so this share of the bound is negligible)
-constexpr double EPS_LIGHT = 2.2e-6;
+constexpr double EPS_LIGHT = 1.9e-6;
 // 2 pi (2^19 - 1): below it G = gamma / 2pi has an integer part below 2^19
 constexpr double FUSED_PHASE_GAMMA = 6.283185307179586 * 524287.0;
 constexpr double EPS_HEAVY = 2.0e-13;
