@@ -24,9 +24,12 @@ struct Cand64 {
     uint64_t vi, vf;
 };
 
-MB_DEV Cand64 fold_delta(uint64_t vi, uint64_t vf, double delta) {
+// The fold proper, kept out of line: it runs once per candidate before a kernel's zero loop, and
+// inlined it took two more registers from (and reshuffled) the light tier's loop, which ran 5%
+// slower (1.355 against 1.289 ms for the light tier alone at 4,096 x 466,659).
+static __device__ __noinline__ Cand64 fold_delta_nonzero(uint64_t vi, uint64_t vf, double delta) {
     Cand64 c{vi, vf};
-    if (delta != 0.0) {
+    {
         // delta = M 2^(e - 53) exactly (|M| < 2^53), so delta 2^64 = M 2^sh: its 128-bit magnitude,
         // rounded to the nearest integer (half up) when sh < 0, is added to or subtracted from v.
         // Every step is exact (1 + delta, say, would round for small negative delta).
@@ -55,6 +58,11 @@ MB_DEV Cand64 fold_delta(uint64_t vi, uint64_t vf, double delta) {
         }
     }
     return c;
+}
+
+MB_DEV Cand64 fold_delta(uint64_t vi, uint64_t vf, double delta) {
+    if (delta == 0.0) return Cand64{vi, vf};
+    return fold_delta_nonzero(vi, vf, delta);
 }
 
 // ---------------------------------------------------------------- exact phase

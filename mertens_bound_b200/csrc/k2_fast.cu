@@ -422,22 +422,40 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
     return MB_OK;
 }
 
-// Opt every kernel that holds the heavy table into HEAVY_DSMEM bytes of dynamic shared memory (once
-// per device; the attribute is per device and function).  Plans call it when they are built, so
-// a first launch inside a stream capture finds it done.
+// Opt every kernel that holds the heavy table into HEAVY_DSMEM bytes of dynamic shared memory, and
+// give every tier kernel the same shared-memory carveout (the largest): an SM switches its L1 /
+// shared split only when it is idle, so a light CTA could not take an SM that a heavy CTA (with
+// its larger shared-memory need) had just left without one (measured: the two-kernel step
+// 1.726 -> 1.689 ms at 4,096 x 466,659 once the carveouts matched).  Once per device; the attributes are per device and
+// function.  Plans call it when they are built, so a first launch inside a stream capture finds
+// it done.
+template <typename K>
+static int tier_kernel_attributes(K kern, bool heavy_table) {
+    if (heavy_table)
+        MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, HEAVY_DSMEM));
+    MB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+    return MB_OK;
+}
+
 int heavy_smem_attributes() {
     static bool done[64] = {};
     int dev = 0;
     MB_CUDA(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && done[dev]) return MB_OK;
-    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    MB_CUDA(cudaFuncSetAttribute(k2_heavy_kernel, a, HEAVY_DSMEM));
-    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<2, true>, a, HEAVY_DSMEM));
-    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<3, true>, a, HEAVY_DSMEM));
-    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<4, true>, a, HEAVY_DSMEM));
-    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<2, false>, a, HEAVY_DSMEM));
-    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<3, false>, a, HEAVY_DSMEM));
-    MB_CUDA(cudaFuncSetAttribute(k2_tiers_kernel<4, false>, a, HEAVY_DSMEM));
+    MB_TRY(tier_kernel_attributes(k2_heavy_kernel, true));
+    MB_TRY(tier_kernel_attributes(k2_tiers_kernel<2, true>, true));
+    MB_TRY(tier_kernel_attributes(k2_tiers_kernel<3, true>, true));
+    MB_TRY(tier_kernel_attributes(k2_tiers_kernel<4, true>, true));
+    MB_TRY(tier_kernel_attributes(k2_tiers_kernel<2, false>, true));
+    MB_TRY(tier_kernel_attributes(k2_tiers_kernel<3, false>, true));
+    MB_TRY(tier_kernel_attributes(k2_tiers_kernel<4, false>, true));
+    MB_TRY(tier_kernel_attributes(k2_light_kernel<2, 4, true>, false));
+    MB_TRY(tier_kernel_attributes(k2_light_kernel<3, 3, true>, false));
+    MB_TRY(tier_kernel_attributes(k2_light_kernel<4, 2, true>, false));
+    MB_TRY(tier_kernel_attributes(k2_light_kernel<2, 4, false>, false));
+    MB_TRY(tier_kernel_attributes(k2_light_kernel<3, 3, false>, false));
+    MB_TRY(tier_kernel_attributes(k2_light_kernel<4, 2, false>, false));
     if (dev >= 0 && dev < 64) done[dev] = true;
     return MB_OK;
 }
@@ -471,7 +489,7 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
     const TabView tv = view(t);
     const bool heavy = (tiers & 1) && pd.n_heavy > 0;
     const bool light = (tiers & 2) && pd.n_light > 0;
-    if (heavy) MB_TRY(heavy_smem_attributes());
+    if (heavy || light) MB_TRY(heavy_smem_attributes());
     if (pd.one_kernel && heavy && light) {
         MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), s));
         if (ev) MB_CUDA(cudaEventRecord(ev->light0, s));
