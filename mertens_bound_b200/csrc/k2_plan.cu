@@ -197,8 +197,20 @@ int build_items(mb_plan *p, int sms) {
         // coarser light items cost less per term -- both measured)
         if (hz <= 0)
             hz = std::max<int64_t>(128, ((int64_t)(target_h / std::min<int64_t>(CTh, std::max<int64_t>(gr.nc, 1))) + 64) / 128 * 128);
-        if (lz <= 0)
+        // the last light chunks of a group are a quarter of the size, about one round of CTA slots
+        // in all (this group's share of it), so the light items' last wave -- they run largest
+        // first -- ends in small items instead of leaving SMs idle behind full-size ones
+        int64_t small_lz = 0, small_from = le(g);
+        if (lz <= 0) {
             lz = std::max<int64_t>(2048, ((int64_t)(target_l / std::min<int64_t>(CTl, std::max<int64_t>(gr.nc, 1))) + 128) / 256 * 256);
+            const int per_sm = p->light_cpt == 2 ? 4 : (p->light_cpt == 3 ? 3 : 2);
+            const double wg = (double)gr.nc * std::max<int64_t>(0, le(g) - lb(g));
+            const int64_t n_tiles = std::max<int64_t>(1, (gr.nc + CTl - 1) / CTl);
+            const int64_t items = (int64_t)std::ceil((double)sms * per_sm * (Wl > 0 ? wg / Wl : 0.0));
+            small_lz = std::max<int64_t>(256, lz / 4 / 256 * 256);
+            const int64_t span = ((items + n_tiles - 1) / n_tiles) * small_lz;
+            if (span > 0 && le(g) - lb(g) > 2 * span) small_from = le(g) - span;
+        }
         int ch = 0;
         auto emit = [&](int64_t z0, int64_t z1, int tier, int64_t CT, int cpt, std::vector<FastItem> &dst) {
             for (int64_t ct = 0; ct * CT < gr.nc; ++ct) {
@@ -218,8 +230,10 @@ int build_items(mb_plan *p, int sms) {
         };
         for (int64_t z = hb(g); z < he(g); z += hz)
             emit(z, std::min(z + hz, he(g)), 0, CTh, HEAVY_CPT, heavy);
-        for (int64_t z = lb(g); z < le(g); z += lz)
-            emit(z, std::min(z + lz, le(g)), 1, CTl, p->light_cpt, light);
+        for (int64_t z = lb(g); z < small_from; z += lz)
+            emit(z, std::min(z + lz, small_from), 1, CTl, p->light_cpt, light);
+        for (int64_t z = small_from; z < le(g); z += small_lz)
+            emit(z, std::min(z + small_lz, le(g)), 1, CTl, p->light_cpt, light);
         gr.n_chunks = ch;
         p->zero_terms += (double)gr.nc * (std::max<int64_t>(0, he(g) - hb(g)) + std::max<int64_t>(0, le(g) - lb(g)));
         pbase += (int64_t)gr.n_chunks * gr.nc * 3;
