@@ -45,10 +45,11 @@ WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 can
 # `bench.py --profile-case search` (dram__bytes_read.sum + dram__bytes_write.sum), and the
 # executed thread instructions per zero-term of each kernel from the same capture
 # (smsp__inst_executed.sum x 32 / zero-terms): the issue-slot side figure beside the pipe roofline.
-LIGHT_DRAM_BYTES = {2: 16487680, 3: 16464128, 4: 16447232}
-HEAVY_DRAM_BYTES = 2774784
-LIGHT_INST_PER_TERM = {2: 19.75, 3: 20.29, 4: 16.87}
-HEAVY_INST_PER_TERM = 41.04
+LIGHT_DRAM_BYTES = {2: 16539648, 3: 16510464, 4: 16486144}
+HEAVY_DRAM_BYTES = 2747648
+TIERS_DRAM_BYTES = 19289344          # k2_tiers_kernel<4> (both tiers in one launch)
+LIGHT_INST_PER_TERM = {2: 19.76, 3: 20.29, 4: 16.87}
+HEAVY_INST_PER_TERM = 38.65
 # Algorithmic operations per zero-term on each tier's binding pipe:
 #   light tier, XU (MUFU) pipe: one sine and one cosine of the reduced phase;
 #   heavy tier, FP64 pipe: 4 DFMA for the 2^-64 phase products, 1 for the phase sum, 12 for the
@@ -370,7 +371,8 @@ def run_ours(args):
                    if one_kernel else "k2_light_kernel (light tier), inside the concurrent step"),
         "achieved": mufu_achieved / 1e12, "peak": mufu_peak / 1e12, "unit": "T MUFU-op/s",
         "frac": mufu_achieved / mufu_peak,
-        "traffic": LIGHT_DRAM_BYTES[cpt], "traffic_unit": "bytes/launch (ncu dram read+write)",
+        "traffic": TIERS_DRAM_BYTES if one_kernel else LIGHT_DRAM_BYTES[cpt],
+        "traffic_unit": "bytes/launch (ncu dram read+write)",
         "algorithmic": f"{LIGHT_MUFU_PER_TERM} MUFU (sin, cos) per light zero-term",
         "peak_source": "measured live: sin.approx/cos.approx chains (mb_calibrate_pipes)",
         "light_terms": lt, "light_ms_in_step": light_mean,
