@@ -394,7 +394,7 @@ def run_ours(args):
         "heavy_zeros": gi["n_heavy"], "light_form": plan.info()["light_form"],
         "tile_light_cpt": cpt, "tile_nzw_shift": tuned["config"][1], "tile_chunk_scale": tuned["config"][2],
         "schedule": {0: "heavy and light tier kernels concurrently", 1: "one persistent kernel, heavy items first",
-                     2: "one persistent kernel, tiers interleaved"}[tuned["config"][3]],
+                     2: "one persistent kernel, items by cost"}[tuned["config"][3]],
     }
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

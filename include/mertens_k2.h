@@ -188,10 +188,11 @@ int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, double chunk_sca
 /* How the two tiers run: 0 (the default) launches the persistent heavy kernel on a second stream
  * concurrently with the light kernel (one CTA per item); 1 runs every item of both tiers in one
  * persistent kernel (two CTAs per SM pulling heavy items first, then light items, from one
- * counter); 2 is the same kernel with the two tiers' items interleaved in proportion to their
- * estimated cost, so an SM mostly holds one item of each (FP64-bound and XU-bound work side by
- * side).  The results are the same bits in every schedule.  The autotuner tries all three.  No
- * reference counterpart. */
+ * counter); 2 is the same kernel with the items of both tiers in one list ordered by estimated
+ * cost, largest first (a heavy term weighted 2.5 light terms), so the last items to start are the
+ * smallest of either tier.  One-tier runs (mb_plan_run_tiers_dev 1 or 2) use the tier kernels in
+ * every schedule.  The results are the same bits in every schedule.  The autotuner tries all
+ * three.  No reference counterpart. */
 int mb_plan_set_schedule(mb_plan *p, int schedule);
 int mb_plan_schedule(const mb_plan *p, int *schedule);
 /* Restrict every group to the zeros [j0, j1) of its [0, count_below(T)): one shard of a

@@ -466,15 +466,15 @@ static int launch_tiers_one(const TabView &tv, const FastPlanDev &pd, CandView c
     const size_t sm = HEAVY_DSMEM;
     if (pd.fused_phase) {
         switch (pd.light_cpt) {
-            case 2: k2_tiers_kernel<2, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            case 3: k2_tiers_kernel<3, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            default: k2_tiers_kernel<4, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 2: k2_tiers_kernel<2, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
+            case 3: k2_tiers_kernel<3, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
+            default: k2_tiers_kernel<4, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
         }
     } else {
         switch (pd.light_cpt) {
-            case 2: k2_tiers_kernel<2, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            case 3: k2_tiers_kernel<3, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
-            default: k2_tiers_kernel<4, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items, n, pd.groups, pd.counter, pd.partial); break;
+            case 2: k2_tiers_kernel<2, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
+            case 3: k2_tiers_kernel<3, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
+            default: k2_tiers_kernel<4, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
         }
     }
     MB_CUDA(cudaGetLastError());

@@ -35,14 +35,15 @@ constexpr int HEAVY_CPT = 4;     // candidates per thread in the heavy kernel
 // Device side of a plan: items[0, n_heavy) are heavy-tier items (pulled by the persistent
 // heavy kernel), items[n_heavy, n_heavy + n_light) light-tier items (one CTA each).
 struct FastPlanDev {
-    FastItem *items = nullptr;
+    FastItem *items = nullptr;      // heavy items, then light items
+    FastItem *items_one = nullptr;  // the one-kernel schedules' list (items, or a cost-ordered copy)
     FastGroup *groups = nullptr;
     int n_heavy = 0, n_light = 0, n_groups = 0;
     int light_cpt = 4;          // candidates per thread of the light kernel: 2, 3 or 4
     bool fused_phase = false;   // light tier on light_phase32_fused: every zero has gamma below
                                 // FUSED_PHASE_GAMMA, so G's integer part is below 2^19
-    bool one_kernel = false;    // both tiers in k2_tiers_kernel (one persistent kernel, items in
-                                // plan order) instead of the heavy kernel on a side stream beside
+    bool one_kernel = false;    // both tiers in k2_tiers_kernel (one persistent kernel over
+                                // items_one) instead of the heavy kernel on a side stream beside
                                 // the light kernel
     unsigned heavy_grid = 0;
     int *counter = nullptr;

@@ -20,7 +20,8 @@ struct mb_plan {
     std::vector<double> ks, Ts;
     std::vector<int> wslot;        // per group: table weight vector, or -1 for exp(-k gamma^2)
     std::vector<FastGroup> groups;
-    std::vector<FastItem> items;
+    std::vector<FastItem> items;      // heavy items, then light items
+    std::vector<FastItem> items_lpt;  // schedule 2: the same items by estimated cost, both tiers mixed
     std::vector<int64_t> n_T, n_eval, n_heavy;   // zeros below T, zeros evaluated, heavy zeros
     double skip_frac = 0.0;        // share of tol given to skipping the tail of each group
     std::vector<double> err_bound, sum_abs;
@@ -68,6 +69,7 @@ struct mb_plan {
 namespace {
 
 void free_dev(mb_plan *p) {
+    if (p->dev.items_one != p->dev.items) cudaFree(p->dev.items_one);
     cudaFree(p->dev.items);
     cudaFree(p->dev.groups);
     cudaFree(p->dev.counter);
@@ -247,30 +249,20 @@ int build_items(mb_plan *p, int sms) {
     std::stable_sort(light.begin(), light.end(), by_cost);
     p->n_heavy_items = (int)heavy.size();
     if (p->schedule == 2) {
-        // one kernel, tiers interleaved in proportion to their estimated cost (a heavy term costs
-        // ~3.5 light terms), so the two CTAs of an SM mostly hold one item of each tier: the FP64-
-        // bound heavy work and the XU-bound light work share the SM's issue slots
-        auto cost = [](const FastItem &a) { return (a.tier == 0 ? 3.5 : 1.0) * a.nc * (double)(a.z1 - a.z0); };
-        double th = 0, tl = 0, dh = 0, dl = 0;
-        for (const FastItem &a : heavy) th += cost(a);
-        for (const FastItem &a : light) tl += cost(a);
-        p->items.clear();
-        size_t ih = 0, il = 0;
-        while (ih < heavy.size() || il < light.size()) {
-            const bool take_h = il >= light.size() ||
-                                (ih < heavy.size() && dh / std::max(th, 1.0) <= dl / std::max(tl, 1.0));
-            if (take_h) {
-                dh += cost(heavy[ih]);
-                p->items.push_back(heavy[ih++]);
-            } else {
-                dl += cost(light[il]);
-                p->items.push_back(light[il++]);
-            }
-        }
+        // one kernel, every item of both tiers in one list, largest estimated cost first (a heavy
+        // term costs ~2.5 light terms, measured alone): the longest-processing-time order, so the
+        // last items to start, of either tier, are the smallest
+        auto cost = [](const FastItem &a) { return (a.tier == 0 ? 2.5 : 1.0) * a.nc * (double)(a.z1 - a.z0); };
+        p->items_lpt = heavy;
+        p->items_lpt.insert(p->items_lpt.end(), light.begin(), light.end());
+        std::stable_sort(p->items_lpt.begin(), p->items_lpt.end(),
+                         [&](const FastItem &a, const FastItem &b) { return cost(a) > cost(b); });
     } else {
-        p->items = heavy;
-        p->items.insert(p->items.end(), light.begin(), light.end());
+        p->items_lpt.clear();
     }
+    // heavy items then light items: the two-kernel schedule and every one-tier run use this order
+    p->items = heavy;
+    p->items.insert(p->items.end(), light.begin(), light.end());
     p->partial_doubles = (size_t)std::max<int64_t>(pbase, 3);
     return MB_OK;
 }
@@ -290,6 +282,12 @@ int upload(mb_plan *p) {
     p->dev.partial_bytes = p->partial_doubles * sizeof(double);
     if (!p->items.empty())
         MB_CUDA(cudaMemcpy(p->dev.items, p->items.data(), p->items.size() * sizeof(FastItem), cudaMemcpyHostToDevice));
+    p->dev.items_one = p->dev.items;
+    if (!p->items_lpt.empty()) {
+        MB_CUDA(cudaMalloc(&p->dev.items_one, p->items_lpt.size() * sizeof(FastItem)));
+        MB_CUDA(cudaMemcpy(p->dev.items_one, p->items_lpt.data(), p->items_lpt.size() * sizeof(FastItem),
+                           cudaMemcpyHostToDevice));
+    }
     MB_CUDA(cudaMemcpy(p->dev.groups, p->groups.data(), p->groups.size() * sizeof(FastGroup), cudaMemcpyHostToDevice));
     p->dev.n_heavy = p->n_heavy_items;
     p->dev.n_light = (int)p->items.size() - p->n_heavy_items;

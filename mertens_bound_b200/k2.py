@@ -180,8 +180,8 @@ class Plan:
 
     def set_schedule(self, schedule: int):
         """0: the two tier kernels run concurrently (heavy persistent kernel on a side stream);
-        1: one persistent kernel runs both tiers' items, heavy first; 2: the same kernel with the
-        two tiers' items interleaved in proportion to their cost."""
+        1: one persistent kernel runs both tiers' items, heavy first; 2: the same kernel with all
+        items ordered by estimated cost, largest first."""
         check(_lib.lib().mb_plan_set_schedule(self.handle, int(schedule)))
 
     def schedule(self) -> int:

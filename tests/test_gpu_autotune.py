@@ -49,6 +49,34 @@ def test_schedules_give_the_same_bits(gpu, small_table, cpt):
         assert np.array_equal(x, y) and np.array_equal(x, z) and np.array_equal(x, w)
 
 
+def test_one_tier_runs_in_every_schedule(gpu, small_table):
+    """mb_plan_run_tiers_dev with one tier gives that tier's terms only, whatever the schedule (the
+    cost-ordered schedule keeps its own item list for the one-kernel run)."""
+    import torch
+    from mertens_bound_b200._lib import check, lib
+    dev = torch.device("cuda", 0)
+    cd = synth.make_candidates(600, seed=35)
+    vi = torch.from_numpy(cd.v_int.view(np.int64).copy()).to(dev)
+    vf = torch.from_numpy(cd.v_frac.view(np.int64).copy()).to(dev)
+    out = torch.empty(3, 3, 600, dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    res = {}
+    with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [600], [3e-9], [math.inf], tol=1e-8) as plan:
+        for sched in (0, 1, 2):
+            plan.set_schedule(sched)
+            for i, tiers in enumerate((1, 2, 3)):
+                o = out[i]
+                check(lib().mb_plan_run_tiers_dev(plan.handle, tiers, vi.data_ptr(), vf.data_ptr(), None,
+                                                  o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr(), s))
+            torch.cuda.synchronize(dev)
+            res[sched] = out.cpu().numpy().copy()
+        eb = plan.group_info(0)["err_bound"]
+    for sched in (1, 2):
+        assert np.array_equal(res[sched], res[0])
+    o = res[0]
+    assert np.max(np.abs(o[0, 0] + o[1, 0] - o[2, 0])) <= 1e-3 * eb
+
+
 def test_kernel_timing_hook(gpu, small_table):
     """mb_plan_kernel_timing / mb_plan_kernel_times: per-run tier kernel durations under each
     schedule (one launch under the one-kernel schedules, reported as the light time)."""
