@@ -168,8 +168,10 @@ int mb_plan_destroy(mb_plan *p);
 int mb_plan_set_skip(mb_plan *p, double skip_frac);
 /* Autotuner: times every tile configuration (light_cpt in {2, 3, 4} x nzw_shift in {0, 1} x
  * chunk_scale in {0.5, 1, 2}, in that nesting order; timings, nullable, receives the 18 median
- * times in ms) with mb_plan_time(reps) and applies the fastest.  The Python layer caches the
- * choice per GPU and workload class.  No reference counterpart (its evaluator has no tunables). */
+ * times in ms) with mb_plan_time(reps) under the plan's current schedule and applies the fastest.
+ * The Python layer runs it under each schedule (mb_plan_set_schedule), keeps the fastest pair and
+ * caches the choice per GPU and workload class.  No reference counterpart (its evaluator has no
+ * tunables). */
 int mb_plan_autotune(mb_plan *p, int reps, int *light_cpt, int *nzw_shift, double *chunk_scale, double *best_ms,
                      double *timings);
 /* A-priori bounds of the absolute error of group g's outputs: K2 (the bound of
