@@ -384,6 +384,10 @@ def run_ours(args):
         "heavy_traffic": HEAVY_DRAM_BYTES,
         "step_xu_frac": LIGHT_MUFU_PER_TERM * lt / (ms_per_step * 1e-3) / mufu_peak,
         "step_fp64_frac": HEAVY_FP64_PER_TERM * ht / (ms_per_step * 1e-3) / dfma_peak,
+        # both tiers' algorithmic work at their pipes' peaks, one after the other, over the step:
+        # the fraction of a step whose pipes could not overlap
+        "step_pipe_time_frac": (LIGHT_MUFU_PER_TERM * lt / mufu_peak + HEAVY_FP64_PER_TERM * ht / dfma_peak)
+                               / (ms_per_step * 1e-3),
         "issue_frac_side": (LIGHT_INST_PER_TERM[cpt] * lt + HEAVY_INST_PER_TERM * ht) / (ms_per_step * 1e-3)
                            / ffma_peak,
         "hbm_frac_side": (LIGHT_DRAM_BYTES[cpt] + HEAVY_DRAM_BYTES) / (ms_per_step * 1e-3) / 1e9 / hbm_peak()[0],
