@@ -135,7 +135,7 @@ int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamma, const do
  * n_heavy chosen so that the a-priori worst-case error bound stays <= tol: the first n_heavy
  * zeros (the heavy tier) are summed in FP64 (64-bit phase, table sine/cosine with FP64
  * polynomials), the rest (the light tier) with a 32-bit phase, MUFU sine/cosine and FP32
- * accumulators that are added into FP64 partial sums every 16 terms.  Each tier is one kernel
+ * accumulators that are added into FP64 partial sums every 32 terms.  Each tier is one kernel
  * over the work items of every group: the heavy kernel is persistent (two CTAs per SM pull items
  * from a counter) and runs on a second stream concurrently with the light kernel (one CTA per
  * item); a deterministic reduction adds the partial sums.  mb_plan_run replays a captured CUDA

@@ -59,7 +59,7 @@ struct __align__(16) ZHeavy {   // 96 B
 constexpr int FAST_THREADS = 256;
 constexpr int LIGHT_TILE = 256;
 constexpr int HEAVY_TILE = 128;
-constexpr int LIGHT_FLUSH = 16;
+constexpr int LIGHT_FLUSH = 32;
 // shared memory: the staged tile, reused after the tile loop for the cross-warp reduction
 constexpr int FAST_SMEM = 24576;
 static_assert(FAST_SMEM >= LIGHT_TILE * sizeof(ZLight), "light tile");
