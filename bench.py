@@ -45,11 +45,11 @@ WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 can
 # `bench.py --profile-case search` (dram__bytes_read.sum + dram__bytes_write.sum), and the
 # executed thread instructions per zero-term of each kernel from the same capture
 # (smsp__inst_executed.sum x 32 / zero-terms): the issue-slot side figure beside the pipe roofline.
-LIGHT_DRAM_BYTES = {2: 16539648, 3: 16510464, 4: 16486144}
-HEAVY_DRAM_BYTES = 2747648
-TIERS_DRAM_BYTES = 19289344          # k2_tiers_kernel<4> (both tiers in one launch)
-LIGHT_INST_PER_TERM = {2: 19.76, 3: 20.29, 4: 16.87}
-HEAVY_INST_PER_TERM = 38.65
+LIGHT_DRAM_BYTES = {2: 16468224, 3: 16438016, 4: 16415488}
+HEAVY_DRAM_BYTES = 2825472
+TIERS_DRAM_BYTES = 19296000          # k2_tiers_kernel<4> (both tiers in one launch)
+LIGHT_INST_PER_TERM = {2: 19.32, 3: 19.86, 4: 16.54}
+HEAVY_INST_PER_TERM = 38.64
 # Algorithmic operations per zero-term on each tier's binding pipe:
 #   light tier, XU (MUFU) pipe: one sine and one cosine of the reduced phase;
 #   heavy tier, FP64 pipe: 4 DFMA for the 2^-64 phase products, 1 for the phase sum, 12 for the
