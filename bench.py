@@ -45,18 +45,19 @@ WORKLOAD = ("search_scoring: all 466,659 synthetic zeros below T0=3e5, 4,096 can
 # `bench.py --profile-case search` (dram__bytes_read.sum + dram__bytes_write.sum), and the
 # executed thread instructions per zero-term of each kernel from the same capture
 # (smsp__inst_executed.sum x 32 / zero-terms): the issue-slot side figure beside the pipe roofline.
-LIGHT_DRAM_BYTES = {2: 16468224, 3: 16438016, 4: 16415488}
-HEAVY_DRAM_BYTES = 2825472
-TIERS_DRAM_BYTES = 19296000          # k2_tiers_kernel<4> (both tiers in one launch)
+LIGHT_DRAM_BYTES = {2: 16468736, 3: 16439040, 4: 16414976}
+HEAVY_DRAM_BYTES = 2827264
+TIERS_DRAM_BYTES = 19178240          # k2_tiers_kernel<4> (both tiers in one launch)
 LIGHT_INST_PER_TERM = {2: 19.32, 3: 19.86, 4: 16.54}
-HEAVY_INST_PER_TERM = 38.64
+HEAVY_INST_PER_TERM = 39.39
 # Algorithmic operations per zero-term on each tier's binding pipe:
 #   light tier, XU (MUFU) pipe: one sine and one cosine of the reduced phase;
-#   heavy tier, FP64 pipe: 4 DFMA for the 2^-64 phase products, 1 for the phase sum, 12 for the
-#   table sine/cosine (index, remainder, r^2, two short polynomials, two rotations) and 3 FMA
-#   accumulations of K2, dK2/ddelta, dK2/dk.
+#   heavy tier, FP64 pipe: 4 DFMA for the 2^-64-turn phase products, 1 add onto the rounding
+#   constant, 1 FMA for the exact table remainder, 8 for the table sine/cosine (r^2, the sine
+#   polynomial and product, the cosine product, two 2-FMA rotations) and 3 FMA accumulations of
+#   K2, dK2/ddelta, dK2/dk.
 LIGHT_MUFU_PER_TERM = 2
-HEAVY_FP64_PER_TERM = 20
+HEAVY_FP64_PER_TERM = 17
 REF_SAMPLE_CANDS = 64
 
 
@@ -398,7 +399,8 @@ def run_ours(args):
         "heavy_zeros": gi["n_heavy"], "light_form": plan.info()["light_form"],
         "tile_light_cpt": cpt, "tile_nzw_shift": tuned["config"][1], "tile_chunk_scale": tuned["config"][2],
         "schedule": {0: "heavy and light tier kernels concurrently", 1: "one persistent kernel, heavy items first",
-                     2: "one persistent kernel, items by cost"}[tuned["config"][3]],
+                     2: "one persistent kernel, items by cost",
+                     3: "one persistent kernel, one queue per tier"}[tuned["config"][3]],
     }
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -192,9 +192,11 @@ int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, double chunk_sca
  * persistent kernel (two CTAs per SM pulling heavy items first, then light items, from one
  * counter); 2 is the same kernel with the items of both tiers in one list ordered by estimated
  * cost, largest first (a heavy term weighted 2.5 light terms), so the last items to start are the
- * smallest of either tier.  One-tier runs (mb_plan_run_tiers_dev 1 or 2) use the tier kernels in
- * every schedule.  The results are the same bits in every schedule.  The autotuner tries all
- * three.  No reference counterpart. */
+ * smallest of either tier; 3 is the same kernel with one queue per tier: the first CTA on each SM
+ * pulls heavy items, the second light items, and a CTA whose queue is empty takes the other's.
+ * One-tier runs (mb_plan_run_tiers_dev 1 or 2) use the tier kernels in every schedule.  The
+ * results are the same bits in every schedule.  The autotuner tries all four.  No reference
+ * counterpart. */
 int mb_plan_set_schedule(mb_plan *p, int schedule);
 int mb_plan_schedule(const mb_plan *p, int *schedule);
 /* Restrict every group to the zeros [j0, j1) of its [0, count_below(T)): one shard of a
@@ -239,7 +241,7 @@ int mb_calibrate_pipes(int device, double *ffma_per_s, double *mufu_per_s, doubl
 int mb_plan_kernel_timing(mb_plan *p, int n_slots);
 /* The light and heavy kernel times (ms) of the last min(n, n_slots, runs) timed runs, oldest
  * first, in light_ms / heavy_ms (-1 where that tier did not run); *n_out = how many.  Under a
- * one-kernel schedule (mb_plan_set_schedule 1 or 2) a run of both tiers is one launch: its time
+ * one-kernel schedule (mb_plan_set_schedule 1, 2 or 3) a run of both tiers is one launch: its time
  * is in light_ms and heavy_ms is -1.  Waits for those runs' events. */
 int mb_plan_kernel_times(mb_plan *p, int n, double *light_ms, double *heavy_ms, int *n_out);
 

@@ -7,7 +7,8 @@ The search space is the plan-wide tile configuration (mb_plan_configure) under e
   nzw_shift    extra doublings of the warps that split one candidate set's zeros
   chunk_scale  work-item size relative to the automatic choice
   schedule     0: the two tier kernels concurrently, 1: one persistent kernel for both tiers,
-               2: the same with all items ordered by estimated cost
+               2: the same with all items ordered by estimated cost, 3: the same with one queue
+               per tier (one CTA of each tier per SM)
 Every configuration is timed on the device (median of `reps` runs, synthetic candidates) and the
 fastest one is applied.  Results are cached per (GPU name, workload class) in a JSON file
 ($MB_AUTOTUNE_CACHE, default ~/.cache/mertens_k2/autotune.json); a workload class buckets the
@@ -23,7 +24,7 @@ import threading
 from . import k2
 
 SPACE = [(cpt, shift, scale) for cpt in (2, 3, 4) for shift in (0, 1) for scale in (0.5, 1.0, 2.0)]
-SCHEDULES = (0, 1, 2)
+SCHEDULES = (0, 1, 2, 3)
 _lock = threading.Lock()
 
 

@@ -3,7 +3,7 @@
 // Each group (k, T, a range of candidates) splits its zeros [0, n_T) at a boundary n_h chosen
 // from an a-priori error bound (host, k2_plan.cu):
 //   heavy tier  j <  n_h : 64-bit phase (3 IMAD.lo + 4 DFMA + 4 FFMA, error ~2^-48 turn), sin/cos
-//                          from a 1024-entry table rotated by short FP64 polynomials, FP64
+//                          from a 2048-entry table rotated by short FP64 polynomials, FP64
 //                          accumulation.                                  -> k2_heavy_kernel
 //   light tier  j >= n_h : 32-bit phase (3 IMAD.lo + 4 DFMA in two chains; 2 IMAD.lo + 3 DFMA
 //                          when every zero has gamma < 3.29e6, light_phase32_fused), MUFU sin/cos
@@ -49,10 +49,10 @@ struct __align__(16) ZLightF {  // 48 B: the light record of light_phase32_fused
 };
 
 struct __align__(16) ZHeavy {   // 96 B
-    uint32_t b0, b1, gi, psi_hi; // psi_hi = top 32 bits of arg(c)/2pi 2^64
-    double b0s, c1s, gis, b1s;   // limb 2^-64
-    float c0f, c1f, b0f, b1f;    // limb 2^-96 (FP32: these products need 2^-18 relative)
-    float psi_lo, pad0;          // low 32 bits of arg(c)/2pi 2^64, times 2^-64
+    uint32_t b0, b1, gi, psi_hi; // psi_hi = top 32 bits of arg(c)/2pi 2^64, plus 2^20 (half a table step)
+    double b0s, c1s, gis, b1s;   // limb 2^-32
+    float c0f, c1f, b0f, b1f;    // limb 2^-64 (FP32: these products need 2^-18 relative)
+    float psi_lo, pad0;          // low 32 bits of arg(c)/2pi 2^64, times 2^-32
     double a, b, d;
 };
 
@@ -120,20 +120,16 @@ MB_DEV void light_tile(const void *tile_v, int nt, int zl, int ZL, const CandReg
     flush();
 }
 
-// sin/cos(2 pi y) for any y (turns): y = q/2048 + r with |r| <= 2^-12 (exact), the table
-// entry (cos, sin)(2 pi q/2048) rotated by r: sin(2 pi r) = r (2pi - (2pi)^3 r^2 / 6) (truncation
-// 7e-17) and cos(2 pi r) - 1 = C r^2 with C the minimax constant on |r| <= 2^-12 (-(2pi)^2/2 +
-// 3.2e-6: error 3.96e-14, computed with mpmath), so the cosine costs one product.
+// sin/cos(2 pi (q/2048 + r)) for |r| <= 2^-12 turn: the table entry (cos, sin)(2 pi q/2048)
+// rotated by r: sin(2 pi r) = r (2pi - (2pi)^3 r^2 / 6) (truncation 7e-17) and
+// cos(2 pi r) - 1 = C r^2 with C the minimax constant on |r| <= 2^-12 (-(2pi)^2/2 + 3.2e-6:
+// error 3.96e-14, computed with mpmath), so the cosine costs one product.
 constexpr int HEAVY_TAB = 2048;
 constexpr int HEAVY_TAB_BYTES = HEAVY_TAB * (int)sizeof(double2);
-MB_DEV void sincos_turns_tab(double y, const double2 *tab, double &sn, double &cs) {
-    const double m = fma(y, (double)HEAVY_TAB, MB_MAGIC);
-    const int q = __double2loint(m) & (HEAVY_TAB - 1);
-    const double r = fma(-1.0 / HEAVY_TAB, m - MB_MAGIC, y);
+MB_DEV void sincos_rotate(double2 T, double r, double &sn, double &cs) {
     const double u = r * r;
     const double s = r * fma(u, -41.341702240399755, 6.283185307179586);     // sin(2 pi r)
     const double cm1 = u * -19.739205595594533;                            // cos(2 pi r) - 1
-    const double2 T = tab[q];
     cs = fma(T.x, cm1, fma(-T.y, s, T.x));
     sn = fma(T.y, cm1, fma(T.x, s, T.y));
 }
@@ -152,6 +148,17 @@ MB_DEV double2 *heavy_table_init(unsigned char *dsm) {
     return tab;
 }
 
+// 1.5 2^35: a sum x in [0, 2^34) units of 2^-32 turn added to it rounds to a multiple of 2^-17
+// unit, and the low 51 mantissa bits of the result hold x 2^17.
+constexpr double HEAVY_MAGIC = 51539607552.0;
+
+// The heavy term's phase in units of 2^-32 turn, T = L + F mod 2^32 with
+//   L = a1 b0 + a0 b1 + d1 gI + psi_hi (+ 2^20)     exact mod 2^32 (IMAD.lo)
+//   F = (a0 b0 + a1 c1 + d0 gI + d1 b1) 2^-32       < 2^34, two FP64 chains, one on HEAVY_MAGIC
+//     + (a1 c0 + a0 c1 + d1 b0 + d0 b1) 2^-64 + psi_lo   < 5, FP32
+// (error <= 2^-16 unit = 2^-48 turn).  The bits of HEAVY_MAGIC + F plus L 2^17 (one 64-bit
+// integer multiply-add) are T 2^17: bits [38, 49) are the table index q, bits [0, 38) the offset
+// R, and r = R 2^-49 - 2^-12 turn is exact as (2^52 + R) 2^-49 - (8 + 2^-12).
 template <int CPT>
 MB_DEV void heavy_tile(const ZHeavy *tile, int nt, int zl, int ZL, const CandRegs (&cr)[CPT],
                        double (&acc)[CPT][3], const double2 *tab) {
@@ -159,16 +166,19 @@ MB_DEV void heavy_tile(const ZHeavy *tile, int nt, int zl, int ZL, const CandReg
         const ZHeavy z = tile[jj];
 #pragma unroll
         for (int i = 0; i < CPT; ++i) {
-            uint32_t lo32 = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi + z.psi_hi;
-            // the 2^-96 products (< 2^-30 turn in all) in FP32, seeded with psi's low word
+            const uint32_t L = cr[i].a1 * z.b0 + cr[i].a0 * z.b1 + cr[i].d1 * z.gi + z.psi_hi;
             const float low = fmaf(__uint2float_rn(cr[i].a1), z.c0f, fmaf(__uint2float_rn(cr[i].a0), z.c1f,
                               fmaf(__uint2float_rn(cr[i].d1), z.b0f,
                               fmaf(__uint2float_rn(cr[i].d0), z.b1f, z.psi_lo))));
-            double F = fma(cr[i].A0, z.b0s, fma(cr[i].A1, z.c1s, fma(cr[i].D0, z.gis,
-                       fma(cr[i].D1, z.b1s, (double)low))));
-            double y = fma(u32_to_f64(lo32), TWO_M32, F);
+            const double p1 = fma(cr[i].A0, z.b0s, fma(cr[i].A1, z.c1s, (double)low));
+            const double p2 = fma(cr[i].D0, z.gis, fma(cr[i].D1, z.b1s, HEAVY_MAGIC));
+            const unsigned long long w =
+                (unsigned long long)L * 131072ull + (unsigned long long)__double_as_longlong(p1 + p2);
+            const uint32_t wh = (uint32_t)(w >> 32);
+            const double r = fma(__hiloint2double((int)((wh & 0x3Fu) | 0x43300000u), (int)(uint32_t)w),
+                                 1.7763568394002505e-15, -8.000244140625);        // 2^-49, 8 + 2^-12
             double sn, cs;
-            sincos_turns_tab(y, tab, sn, cs);
+            sincos_rotate(tab[(wh >> 6) & (HEAVY_TAB - 1)], r, sn, cs);
             acc[i][0] = fma(z.a, cs, acc[i][0]);
             acc[i][1] = fma(z.b, sn, acc[i][1]);
             acc[i][2] = fma(z.d, cs, acc[i][2]);
@@ -215,17 +225,17 @@ MB_DEV void stage_heavy(const TabView &t, int64_t j, double k, const double *w, 
     double a = 2.0 * t.alpha[j] * (w ? w[j] : exp(-k * g * g));
     uint32_t c0 = t.g0[j], c1 = t.g1[j], b0 = t.g2[j], b1 = t.g3[j], gi = t.g4[j];
     r.b0 = b0; r.b1 = b1; r.gi = gi;
-    r.b0s = u32_to_f64(b0) * TWO_M64;
-    r.c1s = u32_to_f64(c1) * TWO_M64;
-    r.gis = u32_to_f64(gi) * TWO_M64;
-    r.b1s = u32_to_f64(b1) * TWO_M64;
-    r.c0f = (float)(u32_to_f64(c0) * TWO_M96);
-    r.c1f = (float)(u32_to_f64(c1) * TWO_M96);
-    r.b0f = (float)(u32_to_f64(b0) * TWO_M96);
-    r.b1f = (float)(u32_to_f64(b1) * TWO_M96);
+    r.b0s = u32_to_f64(b0) * TWO_M32;
+    r.c1s = u32_to_f64(c1) * TWO_M32;
+    r.gis = u32_to_f64(gi) * TWO_M32;
+    r.b1s = u32_to_f64(b1) * TWO_M32;
+    r.c0f = (float)(u32_to_f64(c0) * TWO_M64);
+    r.c1f = (float)(u32_to_f64(c1) * TWO_M64);
+    r.b0f = (float)(u32_to_f64(b0) * TWO_M64);
+    r.b1f = (float)(u32_to_f64(b1) * TWO_M64);
     const uint64_t ps = t.psi[j];
-    r.psi_hi = (uint32_t)(ps >> 32);
-    r.psi_lo = (float)(u32_to_f64((uint32_t)ps) * TWO_M64);
+    r.psi_hi = (uint32_t)(ps >> 32) + (1u << 20);
+    r.psi_lo = (float)(u32_to_f64((uint32_t)ps) * TWO_M32);
     r.pad0 = 0.f;
     r.a = a;
     r.b = -a * g;
@@ -345,20 +355,46 @@ k2_light_kernel(TabView t, CandView c, const FastItem *items, const FastGroup *g
     light_item<CPT, FUSED>(it, groups[it.group], t, c, partial, smem);
 }
 
-// Both tiers in one persistent kernel: two CTAs per SM pull items from one counter, the heavy
-// items first (largest first), then the light items (largest first), so the SMs stay busy to the
+// Both tiers in one persistent kernel: two CTAs per SM pull items, so the SMs stay busy to the
 // end without a second launch.  The light part runs at the heavy part's register budget
 // (launch bounds 256 x 2: at most 128 registers per thread).
+//   n_first == 0: one queue, counter[0] over items[0, n_items) (heavy items first or a
+//                 cost-ordered list of both tiers);
+//   n_first  > 0: paired -- the first CTA to arrive on an SM (counter[2 + smid]) pulls heavy
+//                 items [0, n_first) from counter[0], the second light items [n_first, n_items)
+//                 from counter[1], so each SM runs one CTA of each tier (FP64 pipe beside XU
+//                 pipe); a CTA whose queue is empty takes the other one's.
 template <int CPT, bool FUSED>
 __global__ void __launch_bounds__(FAST_THREADS, 2)
-k2_tiers_kernel(TabView t, CandView c, const FastItem *items, int n_items, const FastGroup *groups, int *counter,
-                double *partial) {
+k2_tiers_kernel(TabView t, CandView c, const FastItem *items, int n_items, int n_first, const FastGroup *groups,
+                int *counter, double *partial) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_item;
+    __shared__ int s_item, s_queue;
     const double2 *s_tab = heavy_table_init(smem);
+    if (threadIdx.x == 0 && n_first > 0) {
+        unsigned smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        s_queue = smid < TIERS_COUNTERS - 2 ? atomicAdd(&counter[2 + smid], 1) & 1 : (int)(blockIdx.x & 1);
+    }
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) {
+            if (n_first == 0) {
+                s_item = atomicAdd(counter, 1);
+            } else {
+                int idx = n_items;
+                for (int tries = 0; tries < 2; ++tries) {
+                    const int q = s_queue;
+                    const int k = atomicAdd(&counter[q], 1);
+                    if (q == 0 ? k < n_first : n_first + k < n_items) {
+                        idx = q == 0 ? k : n_first + k;
+                        break;
+                    }
+                    s_queue = q ^ 1;
+                }
+                s_item = idx;
+            }
+        }
         __syncthreads();
         const int idx = s_item;
         if (idx >= n_items) break;
@@ -461,22 +497,26 @@ int heavy_smem_attributes() {
 }
 
 static int launch_tiers_one(const TabView &tv, const FastPlanDev &pd, CandView c, cudaStream_t s) {
-    const unsigned grid = pd.heavy_grid;
+    const unsigned grid = pd.tiers_grid;
     const int n = pd.n_heavy + pd.n_light;
+    const int nf = pd.paired ? pd.n_heavy : 0;
     const size_t sm = HEAVY_DSMEM;
+#define MB_TIERS(C, F) k2_tiers_kernel<C, F><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, nf, pd.groups, \
+                                                                         pd.counter, pd.partial)
     if (pd.fused_phase) {
         switch (pd.light_cpt) {
-            case 2: k2_tiers_kernel<2, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
-            case 3: k2_tiers_kernel<3, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
-            default: k2_tiers_kernel<4, true><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
+            case 2: MB_TIERS(2, true); break;
+            case 3: MB_TIERS(3, true); break;
+            default: MB_TIERS(4, true); break;
         }
     } else {
         switch (pd.light_cpt) {
-            case 2: k2_tiers_kernel<2, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
-            case 3: k2_tiers_kernel<3, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
-            default: k2_tiers_kernel<4, false><<<grid, FAST_THREADS, sm, s>>>(tv, c, pd.items_one, n, pd.groups, pd.counter, pd.partial); break;
+            case 2: MB_TIERS(2, false); break;
+            case 3: MB_TIERS(3, false); break;
+            default: MB_TIERS(4, false); break;
         }
     }
+#undef MB_TIERS
     MB_CUDA(cudaGetLastError());
     return MB_OK;
 }
@@ -491,7 +531,7 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
     const bool light = (tiers & 2) && pd.n_light > 0;
     if (heavy || light) MB_TRY(heavy_smem_attributes());
     if (pd.one_kernel && heavy && light) {
-        MB_CUDA(cudaMemsetAsync(pd.counter, 0, sizeof(int), s));
+        MB_CUDA(cudaMemsetAsync(pd.counter, 0, (pd.paired ? TIERS_COUNTERS : 1) * sizeof(int), s));
         if (ev) MB_CUDA(cudaEventRecord(ev->light0, s));
         MB_TRY(launch_tiers_one(tv, pd, c, s));
         if (ev) MB_CUDA(cudaEventRecord(ev->light1, s));

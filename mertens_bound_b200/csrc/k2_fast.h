@@ -31,6 +31,7 @@ struct FastItem {
 };
 
 constexpr int HEAVY_CPT = 4;     // candidates per thread in the heavy kernel
+constexpr int TIERS_COUNTERS = 2 + 256;   // item counters of one launch: two queues + per-SM arrivals
 
 // Device side of a plan: items[0, n_heavy) are heavy-tier items (pulled by the persistent
 // heavy kernel), items[n_heavy, n_heavy + n_light) light-tier items (one CTA each).
@@ -45,8 +46,10 @@ struct FastPlanDev {
     bool one_kernel = false;    // both tiers in k2_tiers_kernel (one persistent kernel over
                                 // items_one) instead of the heavy kernel on a side stream beside
                                 // the light kernel
-    unsigned heavy_grid = 0;
-    int *counter = nullptr;
+    bool paired = false;        // one_kernel with per-SM roles: one heavy CTA beside one light CTA
+    unsigned heavy_grid = 0;    // CTAs of the heavy kernel
+    unsigned tiers_grid = 0;    // CTAs of k2_tiers_kernel
+    int *counter = nullptr;     // TIERS_COUNTERS item counters
     double *partial = nullptr;
     size_t partial_bytes = 0;   // size of `partial` (a one-tier run clears it first)
 };
@@ -54,7 +57,7 @@ struct FastPlanDev {
 // Per-term worst-case absolute error of cos/sin (times amplitude) in each tier, per unit of
 // amplitude a_j = 2|c_j| w_j:
 //   light: __sinf / __cosf on [-pi, pi] (documented 2^-21.41 / 2^-21.19, so 4.2e-7, their
-//          internal argument scaling included) + the angle (light_angle: int->float 2^-26 turn =
+//          internal argument scaling included) + the angle (int->float 2^-26 turn =
 //          9.4e-8 rad, the FMUL's rounding 2^-23 rad, fl_down(2pi) 4.8e-8 relative = 1.5e-7 rad)
 //          + phase 4.5 2^-32 turn (2.4 with light_phase32_fused; 7e-9 rad): 7.9e-7 in cos / sin;
 //          + amplitude and FFMA roundings (2 2^-24) + FP32 summation over a 32-term flush window

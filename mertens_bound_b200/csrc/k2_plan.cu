@@ -29,7 +29,8 @@ struct mb_plan {
     std::vector<int> shape_nzw;
     std::vector<int64_t> heavy_chunk, light_chunk;
     int light_cpt = 4;
-    int schedule = 0;              // 0: two concurrent tier kernels, 1: one persistent kernel
+    int schedule = 0;              // 0: two concurrent tier kernels, 1: one persistent kernel,
+                                   // 2: the same, cost-ordered, 3: the same, one CTA of each tier per SM
     int nzw_shift = 0;             // extra doublings of the default warps-per-candidate-set split
     double chunk_scale = 1.0;      // multiplies the automatic work-item sizes
     int64_t z_begin = 0, z_end = INT64_MAX;   // zero-range shard of every group (default: all)
@@ -277,7 +278,7 @@ int upload(mb_plan *p) {
     MB_TRY(build_items(p, sms));
     MB_CUDA(cudaMalloc(&p->dev.items, std::max<size_t>(1, p->items.size()) * sizeof(FastItem)));
     MB_CUDA(cudaMalloc(&p->dev.groups, std::max<size_t>(1, p->groups.size()) * sizeof(FastGroup)));
-    MB_CUDA(cudaMalloc(&p->dev.counter, sizeof(int)));
+    MB_CUDA(cudaMalloc(&p->dev.counter, TIERS_COUNTERS * sizeof(int)));
     MB_CUDA(cudaMalloc(&p->dev.partial, p->partial_doubles * sizeof(double)));
     p->dev.partial_bytes = p->partial_doubles * sizeof(double);
     if (!p->items.empty())
@@ -294,10 +295,12 @@ int upload(mb_plan *p) {
     p->dev.n_groups = (int)p->groups.size();
     p->dev.light_cpt = p->light_cpt;
     p->dev.one_kernel = p->schedule >= 1;
+    p->dev.paired = p->schedule == 3;
     p->dev.fused_phase = p->table->h_gamma.empty() || p->table->h_gamma.back() < FUSED_PHASE_GAMMA;
     unsigned hg = 148;
     MB_TRY(heavy_grid_size(p->table->device, &hg));
     p->dev.heavy_grid = std::min<unsigned>(hg, (unsigned)std::max(1, p->n_heavy_items));
+    p->dev.tiers_grid = std::min<unsigned>(hg, (unsigned)std::max<size_t>(1, p->items.size()));
     return MB_OK;
 }
 
@@ -469,12 +472,13 @@ extern "C" int mb_plan_configure(mb_plan *p, int light_cpt, int nzw_shift, doubl
 
 extern "C" int mb_plan_set_schedule(mb_plan *p, int schedule) {
     MB_CHECK_ARG(p, "mb_plan_set_schedule: null plan");
-    MB_CHECK_ARG(schedule >= 0 && schedule <= 2, "mb_plan_set_schedule: schedule=%d (0, 1 or 2)", schedule);
+    MB_CHECK_ARG(schedule >= 0 && schedule <= 3, "mb_plan_set_schedule: schedule=%d (0 .. 3)", schedule);
     MB_TRY(device_guard(p->table->device));
     const bool reorder = (schedule == 2) != (p->schedule == 2);
     p->schedule = schedule;
     if (reorder) return upload(p);     // the item order changes
     p->dev.one_kernel = schedule >= 1;
+    p->dev.paired = schedule == 3;
     free_io(p);                    // the captured graph holds the old launch sequence
     return MB_OK;
 }

@@ -181,7 +181,8 @@ class Plan:
     def set_schedule(self, schedule: int):
         """0: the two tier kernels run concurrently (heavy persistent kernel on a side stream);
         1: one persistent kernel runs both tiers' items, heavy first; 2: the same kernel with all
-        items ordered by estimated cost, largest first."""
+        items ordered by estimated cost, largest first; 3: the same kernel with one queue per
+        tier, the first CTA on each SM pulling heavy items and the second light items."""
         check(_lib.lib().mb_plan_set_schedule(self.handle, int(schedule)))
 
     def schedule(self) -> int:

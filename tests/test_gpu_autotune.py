@@ -1,5 +1,5 @@
-"""The autotuner (mb_plan_autotune under both schedules + the per-workload cache) on a small plan,
-and the two schedules giving the same bits."""
+"""The autotuner (mb_plan_autotune under every schedule + the per-workload cache) on a small plan,
+and the schedules giving the same bits."""
 import math
 
 import numpy as np
@@ -16,8 +16,10 @@ def test_autotune_picks_and_caches(gpu, small_table, tmp_path, monkeypatch):
     with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [1000, 500], [3e-9, 1e-9], [math.inf, 20000.0]) as plan:
         ref, _, _ = plan.run(cd)
         r = autotune.autotune(plan, reps=2)
-        assert not r["cached"] and tuple(r["config"][:3]) in autotune.SPACE and r["config"][3] in (0, 1, 2)
-        assert len(r["timings"]) == 3 * len(autotune.SPACE) and min(r["timings"].values()) == r["ms"]
+        assert not r["cached"] and tuple(r["config"][:3]) in autotune.SPACE and r["config"][3] in autotune.SCHEDULES
+        assert autotune.SCHEDULES == (0, 1, 2, 3)
+        assert len(r["timings"]) == len(autotune.SCHEDULES) * len(autotune.SPACE)
+        assert min(r["timings"].values()) == r["ms"]
         assert plan.schedule() == r["config"][3]
         val, _, _ = plan.run(cd)
         eb = max(plan.group_info(g)["err_bound"] for g in range(2))
@@ -28,8 +30,9 @@ def test_autotune_picks_and_caches(gpu, small_table, tmp_path, monkeypatch):
 
 @pytest.mark.parametrize("cpt", [2, 3, 4])
 def test_schedules_give_the_same_bits(gpu, small_table, cpt):
-    """One persistent kernel for both tiers (in plan order or interleaved) runs the same items with
-    the same per-item arithmetic as the two concurrent kernels, so every output bit agrees."""
+    """One persistent kernel for both tiers (in plan order, interleaved, or one CTA of each tier per
+    SM) runs the same items with the same per-item arithmetic as the two concurrent kernels, so
+    every output bit agrees."""
     cd = synth.make_candidates(700, seed=32)
     cd.delta[:] = np.random.default_rng(33).uniform(-1e-4, 1e-4, cd.n)
     with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [300, 400], [3e-9, 1.5e-10], [math.inf, 20000.0],
@@ -43,10 +46,12 @@ def test_schedules_give_the_same_bits(gpu, small_table, cpt):
         b = plan.run(cd)
         plan.set_schedule(2)
         d = plan.run(cd)
+        plan.set_schedule(3)
+        e = plan.run(cd)
         plan.set_schedule(0)
         c = plan.run(cd)
-    for x, y, z, w in zip(a, b, c, d):
-        assert np.array_equal(x, y) and np.array_equal(x, z) and np.array_equal(x, w)
+    for x, y, z, w, u in zip(a, b, c, d, e):
+        assert np.array_equal(x, y) and np.array_equal(x, z) and np.array_equal(x, w) and np.array_equal(x, u)
 
 
 def test_one_tier_runs_in_every_schedule(gpu, small_table):
@@ -62,7 +67,7 @@ def test_one_tier_runs_in_every_schedule(gpu, small_table):
     s = torch.cuda.current_stream(dev).cuda_stream
     res = {}
     with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [600], [3e-9], [math.inf], tol=1e-8) as plan:
-        for sched in (0, 1, 2):
+        for sched in (0, 1, 2, 3):
             plan.set_schedule(sched)
             for i, tiers in enumerate((1, 2, 3)):
                 o = out[i]
@@ -71,7 +76,7 @@ def test_one_tier_runs_in_every_schedule(gpu, small_table):
             torch.cuda.synchronize(dev)
             res[sched] = out.cpu().numpy().copy()
         eb = plan.group_info(0)["err_bound"]
-    for sched in (1, 2):
+    for sched in (1, 2, 3):
         assert np.array_equal(res[sched], res[0])
     o = res[0]
     assert np.max(np.abs(o[0, 0] + o[1, 0] - o[2, 0])) <= 1e-3 * eb
@@ -92,7 +97,7 @@ def test_kernel_timing_hook(gpu, small_table):
     out = torch.empty(3, 512, dtype=torch.float64, device=dev)
     s = torch.cuda.current_stream(dev).cuda_stream
     with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [512], [3e-9], [math.inf], tol=1e-8) as plan:
-        for sched in (0, 1, 2):
+        for sched in (0, 1, 2, 3):
             plan.set_schedule(sched)
             check(L.mb_plan_kernel_timing(plan.handle, 4))
             for tiers in (3, 3, 1, 2):
