@@ -406,36 +406,43 @@ k2_tiers_kernel(TabView t, CandView c, const FastItem *items, int n_items, int n
     }
 }
 
-// One warp per candidate: lane l sums chunks l, l+32, ... of the candidate's group, then a fixed
-// shuffle tree adds the lanes (deterministic: the order depends only on the chunk count).
+// Eight lanes per candidate, four candidates per warp: lane 4r + q sums the chunks r, r + 8, ...
+// of candidate 4w + q, so the four lanes of one chunk read 96 consecutive bytes; a fixed shuffle
+// tree then adds the eight lanes (deterministic: the order depends only on the chunk count).
+constexpr int REDUCE_LANES = 8;
 __global__ void fast_reduce_kernel(const FastGroup *groups, int n_groups, const double *partial,
                                    int64_t P, double *val, double *dd, double *dk) {
-    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    if (p >= P) return;
-    int lo = 0, hi = n_groups - 1;                 // group containing p (groups sorted by c0)
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (groups[mid].c0 <= p) lo = mid;
-        else hi = mid - 1;
-    }
-    const FastGroup gr = groups[lo];
+    const int r = lane >> 2;
+    const int64_t p = (t >> 5) * 4 + (lane & 3);
+    const bool live = p < P;
     double s0 = 0, s1 = 0, s2 = 0;
-    for (int ch = lane; ch < gr.n_chunks; ch += 32) {
-        const double *o = partial + gr.pbase + ((int64_t)ch * gr.nc + (p - gr.c0)) * 3;
-        s0 += o[0]; s1 += o[1]; s2 += o[2];
+    if (live) {
+        int lo = 0, hi = n_groups - 1;             // group containing p (groups sorted by c0)
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (groups[mid].c0 <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        const FastGroup gr = groups[lo];
+        for (int ch = r; ch < gr.n_chunks; ch += REDUCE_LANES) {
+            const double *o = partial + gr.pbase + ((int64_t)ch * gr.nc + (p - gr.c0)) * 3;
+            s0 += o[0]; s1 += o[1]; s2 += o[2];
+        }
     }
-    for (int off = 16; off > 0; off >>= 1) {
+    for (int off = 16; off >= 4; off >>= 1) {
         s0 += __shfl_xor_sync(0xffffffffu, s0, off);
         s1 += __shfl_xor_sync(0xffffffffu, s1, off);
         s2 += __shfl_xor_sync(0xffffffffu, s2, off);
     }
-    if (lane == 0) {
+    if (live && r == 0) {
         val[p] = s0;
         dd[p] = s1;
         dk[p] = s2;
     }
 }
+static unsigned reduce_blocks(int64_t P) { return (unsigned)(((P + 3) / 4 * 32 + 255) / 256); }
 
 static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cudaStream_t s) {
     if (pd.n_light == 0) return MB_OK;
@@ -535,7 +542,7 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
         if (ev) MB_CUDA(cudaEventRecord(ev->light0, s));
         MB_TRY(launch_tiers_one(tv, pd, c, s));
         if (ev) MB_CUDA(cudaEventRecord(ev->light1, s));
-        fast_reduce_kernel<<<(unsigned)((c.P * 32 + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
+        fast_reduce_kernel<<<reduce_blocks(c.P), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
                                                                          d_val, d_dd, d_dk);
         MB_CUDA(cudaGetLastError());
         return MB_OK;
@@ -565,7 +572,7 @@ int launch_fast(const Table &t, const FastPlanDev &pd, CandView c, double *d_val
         if (ev) MB_CUDA(cudaEventRecord(ev->light1, s));
     }
     if (fork) MB_CUDA(cudaStreamWaitEvent(s, t.ev_join, 0));
-    fast_reduce_kernel<<<(unsigned)((c.P * 32 + 255) / 256), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
+    fast_reduce_kernel<<<reduce_blocks(c.P), 256, 0, s>>>(pd.groups, pd.n_groups, pd.partial, c.P,
                                                                      d_val, d_dd, d_dk);
     MB_CUDA(cudaGetLastError());
     return MB_OK;
