@@ -64,8 +64,9 @@ struct FastPlanDev {
 //          (31 2^-24): 1.97e-6  ->  2.76e-6, held at 2.8e-6.  (A 16-term window gives 1.80e-6
 //          and ~1,000 fewer heavy zeros at the bench workload, but its flush conversions cost
 //          more XU time than those zeros: the step measured 1.4% longer.)
-//   heavy: phase 2^-47 turn (4.5e-14 rad), 2048-entry table + polynomials (cos 3.96e-14, sin
-//          7e-17), FP64 roundings  ->  ~9e-14, held at 2e-13 (loose: the heavy amplitude sum is
+//   heavy: phase 2^-48 turn (2.2e-14 rad; the table index and remainder are exact functions
+//          of the FP64 phase sum's bits), 2048-entry table + polynomials (cos 3.96e-14, sin
+//          7e-17), FP64 roundings  ->  ~7e-14, held at 2e-13 (loose: the heavy amplitude sum is
 //          O(1), so this share of the bound is negligible)
 constexpr double EPS_LIGHT = 2.8e-6;
 // 2 pi (2^19 - 1): below it G = gamma / 2pi has an integer part below 2^19
