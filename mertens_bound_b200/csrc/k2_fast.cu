@@ -426,8 +426,22 @@ __global__ void fast_reduce_kernel(const FastGroup *groups, int n_groups, const 
             else hi = mid - 1;
         }
         const FastGroup gr = groups[lo];
-        for (int ch = r; ch < gr.n_chunks; ch += REDUCE_LANES) {
-            const double *o = partial + gr.pbase + ((int64_t)ch * gr.nc + (p - gr.c0)) * 3;
+        const int64_t stride = (int64_t)gr.nc * 3;
+        const double *o = partial + gr.pbase + (p - gr.c0) * 3 + r * stride;
+        int ch = r;
+        // four chunks per round, all twelve loads issued before the adds (the rounds are
+        // latency-bound otherwise)
+        for (; ch + 3 * REDUCE_LANES < gr.n_chunks; ch += 4 * REDUCE_LANES, o += 4 * REDUCE_LANES * stride) {
+            double x[4][3];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) x[u][q] = o[u * REDUCE_LANES * stride + q];
+            s0 += (x[0][0] + x[1][0]) + (x[2][0] + x[3][0]);
+            s1 += (x[0][1] + x[1][1]) + (x[2][1] + x[3][1]);
+            s2 += (x[0][2] + x[1][2]) + (x[2][2] + x[3][2]);
+        }
+        for (; ch < gr.n_chunks; ch += REDUCE_LANES, o += REDUCE_LANES * stride) {
             s0 += o[0]; s1 += o[1]; s2 += o[2];
         }
     }
