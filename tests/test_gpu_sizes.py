@@ -64,6 +64,13 @@ def test_search_scoring_light_tier_vs_oracle(scoring):
                 first = val
             else:            # the tile width regroups the FP32 sums only: well inside the bound
                 assert np.max(np.abs(val - first)) <= 2 * gi["err_bound"]
+        # the one-kernel schedules (heavy first, by cost, one queue per tier) give the same bits
+        # as the two concurrent kernels at this size
+        last = (val, dd, dk)
+        for sched in (1, 2, 3):
+            plan.set_schedule(sched)
+            for x, y in zip(plan.run(cands), last):
+                assert np.array_equal(x, y), sched
 
 
 def test_search_scoring_split_tiers_add_up(scoring):
