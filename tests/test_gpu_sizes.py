@@ -119,6 +119,11 @@ def test_batched_uneven_groups_vs_oracle(big, oracle):
             gi = _check_bounds(plan, g, np.stack([val[idx], dd[idx], dk[idx]]), ohi)
             assert gi["n_T"] == n_T and gi["err_bound"] <= TOL
             off += c
+        # the same bits under the one-kernel schedules, twelve uneven groups in one launch
+        for sched in (1, 2, 3):
+            plan.set_schedule(sched)
+            for x, y in zip(plan.run(cands), (val, dd, dk)):
+                assert np.array_equal(x, y), sched
 
 
 def test_newton_polish_derivatives_vs_oracle(big, oracle):
