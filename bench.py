@@ -953,8 +953,9 @@ def run_profile_scoring():
 def run_profile_case(args):
     """Fixed cases for ncu captures (no timing, no bench line).
       small   zeros below 1e5, 2,048 candidates: the chosen form (light tier at 4 candidates per
-              thread) args.warmup + args.steps times, then the plain kernel once (~40 MB on the
-              device);
+              thread) args.warmup + args.steps times as two concurrent kernels, once as one
+              persistent kernel with one queue per tier, then the plain kernel once (~40 MB on
+              the device);
       search  the bench workload (zeros below 3e5, 4,096 candidates): the plain kernel once, the
               light tier alone at 2, 3 and 4 candidates per thread, the heavy tier alone, then both
               tiers in one persistent kernel at 4 candidates per thread (~80 MB)."""
@@ -991,6 +992,8 @@ def run_profile_case(args):
         plan.configure(4, 0, 1.0)
         for _ in range(args.warmup + args.steps):
             tiers(3)
+        plan.set_schedule(3)          # both tiers in one persistent kernel, one queue per tier
+        tiers(3)
         plain()
     else:
         plain()
