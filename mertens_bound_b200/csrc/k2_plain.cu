@@ -57,11 +57,39 @@ struct PlainShape {
     int cands_per_cta() const { return (PLAIN_THREADS / 32 / nzw) * (32 >> lpc_log2) * cpt; }
 };
 
+// sin/cos(2 pi hi 2^-64) of the exact 64-bit phase word: the nearest of PLAIN_TAB table angles
+// (the top 11 bits of hi + 2^52) and the remainder r = ((hi + 2^52) mod 2^53 - 2^52) 2^-64 turn,
+// exact in FP64 (|r| <= 2^-12), rotated by
+//   cos(2 pi r) - 1 = r^2 (-2 pi^2 + r^2 2 pi^4 / 3)     (truncation 1.8e-20)
+//   sin(2 pi r)     = r (2 pi - r^2 4 pi^3 / 3)           (truncation 7.1e-17)
+// so the result is within ~4e-16 of the exact values (table entries rounded once, four FMA
+// roundings).  11 FP64 operations and one shared-memory load instead of a 21-operation
+// polynomial pair on the full turn.
+constexpr int PLAIN_TAB = 2048;
+MB_DEV void sincos_phase64_tab(uint64_t hi, const double2 *tab, double &sn, double &cs) {
+    const uint64_t h = hi + (1ull << 52);
+    const int q = (int)(h >> 53);
+    const int32_t rh = (int32_t)((uint32_t)(h >> 32) & 0x1FFFFFu) - (1 << 20);
+    const double r = fma(s32_to_f64(rh), 2.3283064365386963e-10, u32_to_f64((uint32_t)h) * 5.421010862427522e-20);
+    const double u = r * r;
+    const double s = r * fma(u, -41.341702240399755, 6.283185307179586);
+    const double cm1 = u * fma(u, 64.93939402266829, -19.739208802178716);
+    const double2 T = tab[q];
+    cs = fma(T.x, cm1, fma(-T.y, s, T.x));
+    sn = fma(T.y, cm1, fma(T.x, s, T.y));
+}
+
 template <int CPT>
 __global__ void __launch_bounds__(PLAIN_THREADS)
 k2_plain_kernel(TabView t, CandView c, int64_t n_use, int64_t chunk, double k, int lpc_log2,
                 int nzw, double *partial) {
     __shared__ ZRecPlain tile[PLAIN_TILE];
+    __shared__ double2 s_tab[PLAIN_TAB];       // (cos, sin)(2 pi i / PLAIN_TAB); the first tile's
+    for (int i = threadIdx.x; i < PLAIN_TAB; i += PLAIN_THREADS) {   // barrier publishes it
+        double sn, cs;
+        sincospi((double)i * (2.0 / PLAIN_TAB), &sn, &cs);
+        s_tab[i] = make_double2(cs, sn);
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int lpc = 1 << lpc_log2;
     const int cgroup = warp / nzw, zw = warp - cgroup * nzw;
@@ -110,9 +138,8 @@ k2_plain_kernel(TabView t, CandView c, int64_t n_use, int64_t chunk, double k, i
             for (int i = 0; i < CPT; ++i) {
                 uint64_t hi, lo;
                 phase128_exact(v0[i], v1[i], v2[i], v3[i], r.g0, r.g1, r.g2, r.g3, r.g4, hi, lo);
-                double tt = s64_turns_to_f64(hi);
                 double s, co;
-                sincos_turns_half(tt, s, co);
+                sincos_phase64_tab(hi, s_tab, s, co);
                 double wre = fma(r.wcr, co, -r.wci * s);
                 double wim = fma(r.wcr, s, r.wci * co);
                 sv[i] += wre;
@@ -195,9 +222,23 @@ static int sm_count(int device) {
     return n;
 }
 
+// The plain kernel holds 48 KB of static shared memory (tile + sine/cosine table): ask for the
+// largest shared-memory carveout so four CTAs fit on an SM.  Once per device.
+static int plain_kernel_attributes(int device) {
+    static bool done[64] = {};
+    if (device >= 0 && device < 64 && done[device]) return MB_OK;
+    MB_CUDA(cudaFuncSetAttribute(k2_plain_kernel<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+    MB_CUDA(cudaFuncSetAttribute(k2_plain_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+    if (device >= 0 && device < 64) done[device] = true;
+    return MB_OK;
+}
+
 int launch_plain(Table &t, CandView c, int64_t n_use, double k, double *d_val, double *d_dd,
                  double *d_dk, cudaStream_t s, double *d_partial_override, size_t partial_cap) {
     if (c.P == 0) return MB_OK;
+    MB_TRY(plain_kernel_attributes(t.device));
     PlainShape sh = plain_shape(c.P);
     int64_t cta_c = sh.cands_per_cta();
     int64_t n_ctile = (c.P + cta_c - 1) / cta_c;
@@ -343,6 +384,7 @@ extern "C" int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamm
     tv.cim = d_cim;
     tv.n = n_zeros;
     CandView c{d_v_int, d_v_frac, d_delta, P};
+    MB_TRY(plain_kernel_attributes(dev));
     PlainShape sh = plain_shape(P);
     int64_t cta_c = sh.cands_per_cta();
     int64_t n_ctile = (P + cta_c - 1) / cta_c;
