@@ -7,7 +7,9 @@ the exact phase frac(v G + psi) (Python integers and Fractions).
 * heavy tier, heavy_tile (csrc/k2_fast.cu): the whole 2^-32-turn units in IMAD.lo, the FP64
   sums in two chains (one on 1.5 2^35), the FP32 low products, then the table index and the
   remainder from the bits of the FP64 sum plus the whole units times 2^17 (one 64-bit
-  multiply-add); q/2048 + r is within 2^-48 turn of the exact phase for any 64.64 v and 32.128 G.
+  multiply-add); q/2048 + r is within 2^-48 turn of the exact phase for any 64.64 v and 32.128 G;
+* plain kernel, sincos_phase64_tab (csrc/k2_plain.cu): cos/sin of the exact 64-bit phase word
+  from a 2048-entry table and the exact remainder, within 2.5e-16 of mpmath's values.
 
 The phase being reduced is search/path1_eval_fast.cpp:35-46's exact reduction of v gamma / 2pi.
 """
@@ -122,3 +124,32 @@ def test_heavy_remainder_edges():
             q, r = heavy_q_r(vi, vf, G, ps)
             assert 0 <= q < 2048 and abs(r) <= 2.0 ** -12
             assert turn_distance(Fr(q, 2048) + Fr(r), exact_phase(vi, vf, G, ps)) <= Fr(1, 1 << 48)
+
+
+def test_plain_table_sincos_within_2e_16():
+    """k2_plain.cu sincos_phase64_tab on the exact 64-bit phase word: table index from the top
+    11 bits (plus half a step), exact remainder, two short polynomials and the rotation."""
+    import mpmath as mp
+    mp.mp.prec = 120
+    tab = [(float(mp.cos(2 * mp.pi * i / 2048)), float(mp.sin(2 * mp.pi * i / 2048))) for i in range(2048)]
+    rng = random.Random(13)
+    worst = 0.0
+    for it in range(3000):
+        if it % 4:
+            hi = rng.getrandbits(64)
+        else:                            # cell edges: remainder at 0 and at +-half a step
+            hi = ((rng.getrandbits(11) << 53) + rng.choice([0, 1, (1 << 52) - 1, 1 << 52, (1 << 53) - 1])) % (1 << 64)
+        h = (hi + (1 << 52)) % (1 << 64)
+        q = h >> 53
+        rh = ((h >> 32) & 0x1FFFFF) - (1 << 20)
+        r = fma(float(rh), 2.0 ** -32, float(Fr(h & M32, 1 << 64)))
+        assert abs(r) <= 2.0 ** -12
+        u = r * r
+        s = r * fma(u, -41.341702240399755, 6.283185307179586)
+        cm1 = u * fma(u, 64.93939402266829, -19.739208802178716)
+        tx, ty = tab[q]
+        cs = fma(tx, cm1, fma(-ty, s, tx))
+        sn = fma(ty, cm1, fma(tx, s, ty))
+        th = 2 * mp.pi * mp.mpf(hi) / 2 ** 64
+        worst = max(worst, float(abs(cs - mp.cos(th))), float(abs(sn - mp.sin(th))))
+    assert worst <= 2.5e-16, worst
