@@ -114,3 +114,18 @@ def test_kernel_timing_hook(gpu, small_table):
             else:
                 assert all(x == -1 for x in both_heavy)
             check(L.mb_plan_kernel_timing(plan.handle, 0))
+
+
+def test_schedule_argument_checks(gpu, small_table):
+    """mb_plan_set_schedule accepts 0..3 and rejects anything else without changing the plan."""
+    from mertens_bound_b200._lib import K2Error
+    cd = synth.make_candidates(200, seed=36)
+    with k2.ZeroTable.from_data(small_table) as t, k2.Plan(t, [200], [3e-9], [math.inf], tol=1e-8) as plan:
+        ref = plan.run(cd)
+        plan.set_schedule(3)
+        for bad in (-1, 4, 7):
+            with pytest.raises(K2Error):
+                plan.set_schedule(bad)
+        assert plan.schedule() == 3
+        for x, y in zip(plan.run(cd), ref):
+            assert np.array_equal(x, y)
