@@ -122,8 +122,9 @@ int mb_k2_certified_grad_range(mb_table *t, int64_t P, const uint64_t *v_int, co
  * every GPU loading the library keeps until exit, so P <= 349,525 (larger P returns
  * MB_ERR_CAPACITY).  All calls share that array: calls that overlap on the GPU (other streams,
  * other host threads) race on it.  The first call on a device (and the first after that
- * device's context was replaced, e.g. by cudaDeviceReset) looks up the array's address; make it
- * before any stream capture.  Runs on the current device, asynchronously on `stream`. */
+ * device's context was replaced, e.g. by cudaDeviceReset) looks up the array's address and sets
+ * the plain kernel's shared-memory carveout; make it before any stream capture.  Runs on the
+ * current device, asynchronously on `stream`. */
 int mb_k2_plain_noalloc_dev(const uint32_t *d_g, const double *d_gamma, const double *d_cre,
                             const double *d_cim, int64_t n_zeros, int64_t n_use, int64_t P,
                             const uint64_t *d_v_int, const uint64_t *d_v_frac, const double *d_delta,
