@@ -483,9 +483,9 @@ static int launch_light(const TabView &tv, const FastPlanDev &pd, CandView c, cu
 // give every tier kernel the same shared-memory carveout (the largest): an SM switches its L1 /
 // shared split only when it is idle, so a light CTA could not take an SM that a heavy CTA (with
 // its larger shared-memory need) had just left without one (measured: the two-kernel step
-// 1.726 -> 1.689 ms at 4,096 x 466,659 once the carveouts matched).  Once per device; the attributes are per device and
-// function.  Plans call it when they are built, so a first launch inside a stream capture finds
-// it done.
+// 1.726 -> 1.689 ms at 4,096 x 466,659 once the carveouts matched).  Once per device and
+// context (the attributes belong to the context: after a cudaDeviceReset they are set again).
+// Plans call it when they are built, so a first launch inside a stream capture finds it done.
 template <typename K>
 static int tier_kernel_attributes(K kern, bool heavy_table) {
     if (heavy_table)
@@ -496,10 +496,11 @@ static int tier_kernel_attributes(K kern, bool heavy_table) {
 }
 
 int heavy_smem_attributes() {
-    static bool done[64] = {};
+    static void *done_ctx[64] = {};             // the context the attributes were set in
     int dev = 0;
     MB_CUDA(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && done[dev]) return MB_OK;
+    void *ctx = current_context();
+    if (dev >= 0 && dev < 64 && ctx && done_ctx[dev] == ctx) return MB_OK;
     MB_TRY(tier_kernel_attributes(k2_heavy_kernel, true));
     MB_TRY(tier_kernel_attributes(k2_tiers_kernel<2, true>, true));
     MB_TRY(tier_kernel_attributes(k2_tiers_kernel<3, true>, true));
@@ -513,7 +514,7 @@ int heavy_smem_attributes() {
     MB_TRY(tier_kernel_attributes(k2_light_kernel<2, 4, false>, false));
     MB_TRY(tier_kernel_attributes(k2_light_kernel<3, 3, false>, false));
     MB_TRY(tier_kernel_attributes(k2_light_kernel<4, 2, false>, false));
-    if (dev >= 0 && dev < 64) done[dev] = true;
+    if (dev >= 0 && dev < 64) done_ctx[dev] = current_context();
     return MB_OK;
 }
 

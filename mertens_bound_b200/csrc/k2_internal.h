@@ -13,6 +13,9 @@ namespace mb {
 
 // Thread-local last-error message (mb_last_error()).
 void set_error(const char *fmt, ...);
+// The calling thread's current CUDA context (the driver's cuCtxGetCurrent), or null: per-device
+// caches key on it, so they are refreshed after a context is replaced (cudaDeviceReset).
+void *current_context();
 const char *last_error();
 
 // Return-on-error helpers used by every entry point.

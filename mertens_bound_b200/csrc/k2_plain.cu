@@ -222,16 +222,35 @@ static int sm_count(int device) {
     return n;
 }
 
+// The current context handle through the driver's cuCtxGetCurrent (fetched with
+// cudaGetDriverEntryPoint, so the library does not link the driver library itself); null if it
+// cannot be had.
+void *current_context() {
+    typedef int (*ctx_fn)(void **);
+    static ctx_fn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (ctx_fn)f;
+    }();
+    void *ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
 // The plain kernel holds 48 KB of static shared memory (tile + sine/cosine table): ask for the
-// largest shared-memory carveout so four CTAs fit on an SM.  Once per device.
+// largest shared-memory carveout so four CTAs fit on an SM.  Once per device and context.
 static int plain_kernel_attributes(int device) {
-    static bool done[64] = {};
-    if (device >= 0 && device < 64 && done[device]) return MB_OK;
+    static void *done_ctx[64] = {};             // the context the attributes were set in
+    void *ctx = current_context();
+    if (device >= 0 && device < 64 && ctx && done_ctx[device] == ctx) return MB_OK;
     MB_CUDA(cudaFuncSetAttribute(k2_plain_kernel<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared));
     MB_CUDA(cudaFuncSetAttribute(k2_plain_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared));
-    if (device >= 0 && device < 64) done[device] = true;
+    if (device >= 0 && device < 64) done_ctx[device] = current_context();
     return MB_OK;
 }
 
@@ -305,24 +324,6 @@ double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
 void *g_noalloc_ctx[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_noalloc_mu;
 
-// The current context handle through the driver's cuCtxGetCurrent (fetched with
-// cudaGetDriverEntryPoint, so the library does not link the driver library itself); null if it
-// cannot be had.
-void *current_context() {
-    typedef int (*ctx_fn)(void **);
-    static ctx_fn fn = [] {
-        void *f = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            f = nullptr;
-        return (ctx_fn)f;
-    }();
-    void *ctx = nullptr;
-    if (fn && fn(&ctx) != 0) ctx = nullptr;
-    return ctx;
-}
-
 // Device address of the array on the current device (set up once per device and context).
 int noalloc_scratch(double **out) {
     int dev = -1;
@@ -331,7 +332,7 @@ int noalloc_scratch(double **out) {
         mb::set_error("no-allocation scratch: device %d out of range", dev);
         return MB_ERR_ARG;
     }
-    void *ctx = current_context();
+    void *ctx = mb::current_context();
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_addr[dev] || ctx != g_noalloc_ctx[dev]) {
         double *p = nullptr;
@@ -342,7 +343,7 @@ int noalloc_scratch(double **out) {
             return MB_ERR_CUDA;
         }
         g_noalloc_addr[dev] = p;
-        g_noalloc_ctx[dev] = current_context();     // current now, if it was not on entry
+        g_noalloc_ctx[dev] = mb::current_context();     // current now, if it was not on entry
     }
     *out = g_noalloc_addr[dev];
     return MB_OK;
