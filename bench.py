@@ -59,6 +59,7 @@ HEAVY_INST_PER_TERM = 39.39
 LIGHT_MUFU_PER_TERM = 2
 HEAVY_FP64_PER_TERM = 17
 REF_SAMPLE_CANDS = 64
+REF_TIMED_BUDGET_S = 200.0   # the reference arm's timed steps, at most (a bounded sample per step)
 
 
 def parse():
@@ -880,7 +881,9 @@ def hbm_peak():
 def run_reference(args):
     """The reference's own evaluator on the same workload: every timed step scores all 4,096
     candidates over the 466,659 zeros (compute_peak_AB in calls of 64 candidates plus the value and
-    gradient sums); each untimed warm-up step is one such call."""
+    gradient sums) -- fewer, in whole calls, when K such steps would take longer than
+    REF_TIMED_BUDGET_S at the warm-up rate (about 8 s a step on 16 cores); each untimed warm-up
+    step is one such call."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
@@ -889,9 +892,13 @@ def run_reference(args):
     data = synth.make_table_below(T0, seed=1)
     cands = synth.make_candidates(P_PER_GPU, seed=3)
     n_T = data.count_below(T0)
-    reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=max(1, args.warmup))          # warm-up
+    warm_rate = reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=max(1, args.warmup))[0]   # warm-up
+    # every timed step scores all candidates when K steps fit in REF_TIMED_BUDGET_S at the warm-up
+    # rate; otherwise a step is the largest whole number of 64-candidate calls that fits
+    per_step = int(REF_TIMED_BUDGET_S * warm_rate / (max(1, args.steps) * n_T))
+    per_step = max(REF_SAMPLE_CANDS, min(P_PER_GPU, per_step // REF_SAMPLE_CANDS * REF_SAMPLE_CANDS))
     rate, kind, cores, n_steps, secs = reference_rate(data, cands, K_GAUSS, n_T, 0.0, steps=args.steps,
-                                                      per_step=P_PER_GPU)
+                                                      per_step=per_step)
     pf = reference_polish_form(data, cands, K_GAUSS, n_T)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
@@ -900,8 +907,9 @@ def run_reference(args):
         "data": "synthetic (seeded zero table and candidates; no real zeta zeros)",
         "config": workload_config(world, n_T),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"every step: {P_PER_GPU} candidates x {n_T} zeros in calls of "
-                                   f"{REF_SAMPLE_CANDS} (compute_peak_AB + value/grad sums as NumPy dots)",
+                         "sample": f"every step: {per_step} of the {P_PER_GPU} candidates x {n_T} zeros "
+                                   f"in calls of {REF_SAMPLE_CANDS} (compute_peak_AB + value/grad sums as "
+                                   f"NumPy dots)",
                          "nproc": os.cpu_count(), "polish_form_value": pf.get("value"),
                          "polish_form_sample": pf.get("sample", pf.get("unavailable"))},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
